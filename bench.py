@@ -1,0 +1,430 @@
+"""Benchmark: sparse-view DTV reconstruction on the B200 kernels.
+
+Workload (one "step"): a complete 100-iteration DTV (Chambolle-Pock, directional
+TV along x/y/z with per-direction constraint levels) reconstruction of a
+256^3 volume (1 mm voxels) from 64 views over 360 deg on a 384x384 detector
+(1.2 mm pitch), source-origin 500 mm, source-detector 1000 mm, Poisson noise
+at I0 = 1e5. Every iteration runs one forward projection, one FDK-weighted
+backprojection and the fused dual/primal updates; the whole reconstruction is
+one captured CUDA graph.
+
+metric: GRay*samples/s fwd+back = iterations * (forward-projector ray samples
+[exact chord / 1 voxel step, summed over rays] + backprojector voxel*views)
+per second, whole job; recon/s alongside.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Under torchrun (N > 1) every rank reconstructs its own volume (replicas, no
+collective on the data path); the time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "dtv-net_b200"))
+
+METRIC = ("GRay·samples/s fwd+back & unrolled-DTV recon/s vs plain FP32, "
+          "at ≤1e-3 RMSE vs FP64")
+UNIT = "GRay·samples/s"
+
+CFG = dict(nx=256, ny=256, nz=256, voxel=1.0, nu=384, nv=384, pitch=1.2, n_views=64,
+           sod=500.0, sdd=1000.0, iters=100, i0=1e5, seed=2024)
+
+
+def workload_name(c):
+    return (f"sparse-view DTV: {c['nx']}^3 x {c['voxel']:g} mm, {c['n_views']} views/360deg, "
+            f"{c['nu']}x{c['nv']} det @ {c['pitch']:g} mm, SOD {c['sod']:g} SDD {c['sdd']:g}, "
+            f"Poisson I0={c['i0']:g}, {c['iters']} DTV-PDHG iterations")
+
+
+def dist_init():
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def max_over_ranks(x, ws, dev):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        import statistics
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = max(mx, float(parts[1]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[3:7]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- problem
+def make_problem(dev, c, seed):
+    import numpy as np
+    import torch
+
+    import dtvb200
+    from dtvb200.phantom import ellipsoids, poisson_noise
+    ang = np.linspace(0, 360, c["n_views"], endpoint=False)
+    geo = dtvb200.circular(ang, (c["nx"], c["ny"], c["nz"]), (c["voxel"],) * 3,
+                           (c["nu"], c["nv"]), (c["pitch"], c["pitch"]), c["sod"], c["sdd"])
+    truth = ellipsoids((c["nz"], c["ny"], c["nx"]), seed=seed, device=dev)
+    return geo, truth, ang
+
+
+def dtv_params(plan, dev, iters=8):
+    """Step sizes from the spectral radius of BP*A (power method, untimed)."""
+    import torch
+    x = torch.rand(plan.vol_shape(1), device=dev,
+                   generator=torch.Generator(device=dev).manual_seed(5))
+    lam = 1.0
+    for _ in range(iters):
+        y = plan.backward(plan.forward(x))
+        lam = float(torch.linalg.vector_norm(y.double()) / torch.linalg.vector_norm(x.double()))
+        x = y / torch.linalg.vector_norm(y)
+    sigma = 0.9 / lam
+    return dict(sigma=sigma, tau=sigma, mu=1.0, v=(0.5, 0.5, 0.5), quirk=False)
+
+
+def time_steps(fn, steps, stream):
+    import torch
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record(stream)
+    for _ in range(steps):
+        fn()
+    end.record(stream)
+    torch.cuda.synchronize()
+    return start.elapsed_time(end) / 1e3
+
+
+def op_profile(plan, alg, img, sino, dev):
+    """One eager reconstruction with CUDA events around each operator (on the
+    launching stream): average forward / backward / update time per iteration."""
+    import ctypes
+
+    import torch
+
+    import dtvb200
+    from dtvb200 import _lib
+    from dtvb200.geometry import _ptr, _stream
+    key = (tuple(img.shape), img.device.index)
+    st = alg._state[key]
+    prm = alg._params()
+    size = _lib.ivec(plan.geometry.volume_size)
+    stream = torch.cuda.current_stream(dev)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    t_fp = t_bp = t_up = 0.0
+    f, fbar = st["f"], st["fbar"]
+    f.copy_(img)
+    fbar.copy_(img)
+    for k in ("p", "q", "s", "c", "w", "loss"):
+        st[k].zero_()
+    pairs = []
+    for it in range(alg.cascades):
+        if it % alg.t_refresh == 0:
+            st["t"].zero_()
+            _lib.call("dtv_diff_abs_sums", _ptr(f), prm.f_dtype, size, 1, prm.quirk,
+                      _ptr(st["t"]), _stream(dev))
+        e = [ev() for _ in range(4)]
+        e[0].record(stream)
+        plan.forward(fbar, out=st["w"], epilogue=_lib.DTV_EPI_PDHG, g=st["g"], sigma=alg.sigma,
+                     abs_sum=st["loss"][it:it + 1])
+        e[1].record(stream)
+        plan.backward(st["w"], out=st["recon"])
+        e[2].record(stream)
+        _lib.call("dtv_pdhg_dual", _ptr(fbar), _ptr(st["p"]), _ptr(st["q"]), _ptr(st["s"]),
+                  _ptr(st["c"]), size, 1, ctypes.byref(prm), _ptr(st["t"]), _ptr(st["ws"]),
+                  _stream(dev))
+        _lib.call("dtv_pdhg_primal", _ptr(f), _ptr(fbar), _ptr(st["recon"]), _ptr(st["p"]),
+                  _ptr(st["q"]), _ptr(st["s"]), _ptr(st["c"]), size, 1, ctypes.byref(prm),
+                  _ptr(st["ws"]), _stream(dev))
+        e[3].record(stream)
+        pairs.append(e)
+    torch.cuda.synchronize()
+    for e in pairs:
+        t_fp += e[0].elapsed_time(e[1])
+        t_bp += e[1].elapsed_time(e[2])
+        t_up += e[2].elapsed_time(e[3])
+    n = alg.cascades
+    return t_fp / n, t_bp / n, t_up / n
+
+
+# ----------------------------------------------------------------------------- CPU baseline
+def cpu_baseline(c, truth_np, views_per_step=2, steps=1, warmup=0):
+    """The FP64 oracle (OpenMP over all host cores) on a bounded sample of the
+    workload: forward projection and FDK backprojection of `views_per_step`
+    views per step. Returns (GRay*samples/s, cores, sample description, seconds)."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as O
+    ang = np.linspace(0, 360, c["n_views"], endpoint=False)
+    full = O.circular_geometry(ang, (c["nx"], c["ny"], c["nz"]), (c["voxel"],) * 3,
+                               (c["nu"], c["nv"]), (c["pitch"], c["pitch"]), c["sod"], c["sdd"])
+    cores = O.num_threads()
+    vol = np.ascontiguousarray(truth_np, dtype=np.float64)
+    V = c["nx"] * c["ny"] * c["nz"]
+    total_units = 0.0
+    elapsed = 0.0
+    for s in range(warmup + steps):
+        sel = [(s * views_per_step + j) % c["n_views"] for j in range(views_per_step)]
+        g = O.circular_geometry(ang[sel], (c["nx"], c["ny"], c["nz"]), (c["voxel"],) * 3,
+                                (c["nu"], c["nv"]), (c["pitch"], c["pitch"]), c["sod"], c["sdd"])
+        # FDK weight of the full scan (pi / N_full) keeps the sample's arithmetic identical
+        g.og.bp_scale = full.og.bp_scale
+        t0 = time.perf_counter()
+        sino = O.forward(g, vol)
+        O.backward(g, sino)
+        dt = time.perf_counter() - t0
+        if s >= warmup:
+            elapsed += dt
+            total_units += O.fp_samples(g) + V * len(sel)
+    sample = (f"FP64 oracle forward + FDK backprojection of {views_per_step} of "
+              f"{c['n_views']} views per step x {steps} steps (same volume, detector, geometry)")
+    return total_units / elapsed / 1e9, cores, sample, elapsed
+
+
+def run_reference(args):
+    ws, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return 0
+    import torch
+    c = dict(CFG)
+    sys.path.insert(0, os.path.join(REPO, "dtv-net_b200"))
+    from dtvb200.phantom import ellipsoids
+    truth = ellipsoids((c["nz"], c["ny"], c["nx"]), seed=c["seed"], device="cpu").numpy()
+    value, cores, sample, secs = cpu_baseline(c, truth[0, 0], views_per_step=1, steps=args.steps,
+                                              warmup=args.warmup)
+    samples_per_iter = None
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": secs / max(args.steps, 1) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_name(c), "inputs": "seeded ellipsoid phantom"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": ("the reference implements this path only as CUDA kernels (texture "
+                 "references); its CPU path is this FP64 restatement of the same formulas"),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------- ours
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import dtvb200
+    from dtvb200.phantom import poisson_noise
+    ws, rank, local = dist_init()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    c = dict(CFG)
+    if args.small:
+        c.update(nx=64, ny=64, nz=64, nu=96, nv=96, n_views=16, iters=10)
+    geo, truth, _ = make_problem(dev, c, c["seed"] + rank)
+    plan = dtvb200.Plan(geo, max_batch=1, sampler=args.sampler, device=dev)
+    sino_clean = plan.forward(truth)
+    sino = poisson_noise(sino_clean, c["i0"], seed=c["seed"] + rank)
+    prm = dtv_params(plan, dev)
+    alg = dtvb200.DTVCP(plan, c["iters"], t_refresh=10, use_graph=True, **prm)
+    img = torch.zeros(plan.vol_shape(1), device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    # capture (counts the kernels of one replay), then warm up
+    alg.run(img, sino)
+    launches = alg.launches_per_run
+    for _ in range(max(args.warmup - 1, 0)):
+        alg.run(img, sino)
+    fp_samples = plan.fp_samples()
+    V = c["nx"] * c["ny"] * c["nz"]
+    units = c["iters"] * (fp_samples + V * c["n_views"])  # per reconstruction
+
+    # ---- device-resident timing
+    barrier(ws)
+    with ClockSampler(local) as clk:
+        secs = time_steps(lambda: alg.run(img, sino), args.steps, stream)
+    secs = max_over_ranks(secs, ws, dev)
+    barrier(ws)
+    value = ws * units * args.steps / secs / 1e9
+    recon_s = ws * args.steps / secs
+
+    # ---- end to end through the public API with host buffers
+    sino_h = sino.cpu().pin_memory()
+    out_h = torch.empty(plan.vol_shape(1), dtype=torch.float32).pin_memory()
+    res_d = torch.empty(plan.vol_shape(1), device=dev)
+
+    def e2e_step():
+        alg.run(img, sino_h, out=res_d)  # H2D of the sinogram inside run()
+        out_h.copy_(res_d, non_blocking=True)
+
+    e2e_step()
+    barrier(ws)
+    e_secs = max_over_ranks(time_steps(e2e_step, args.steps, stream), ws, dev)
+    e2e_value = ws * units * args.steps / e_secs / 1e9
+
+    # ---- per-operator profile (eager pass with events on the launching stream)
+    t_fp, t_bp, t_up = op_profile(plan, alg, img, sino, dev)
+    n_views, P = c["n_views"], c["n_views"] * c["nu"] * c["nv"]
+    fp_bytes = n_views * V * 4 + P * 4  # one volume pass per view + sinogram write (FP32)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = fp_bytes / (t_fp * 1e-3) / 1e9
+
+    # ---- FP16 storage variant and the plain FP32 single-volume path
+    extra = {}
+    if not args.no_variants:
+        ref_f = alg.run(img, sino)
+        plan16 = dtvb200.Plan(geo, max_batch=1, sampler=args.sampler, stage_f16=True, device=dev)
+        alg16 = dtvb200.DTVCP(plan16, c["iters"], t_refresh=10, use_graph=True,
+                              f_dtype=torch.float16, **prm)
+        alg16.run(img, sino)
+        s16 = time_steps(lambda: alg16.run(img, sino), args.steps, stream)
+        f16 = alg16.run(img, sino)
+        err16 = float(torch.sqrt(((f16 - ref_f).double() ** 2).mean() / (ref_f.double() ** 2).mean()))
+        plain = dtvb200.DTVCP(plan, c["iters"], t_refresh=10, use_graph=False, **prm)
+        plain.run(img, sino)
+        sp = time_steps(lambda: plain.run(img, sino), args.steps, stream)
+        extra = {
+            "fp16_storage": {"value": units * args.steps / s16 / 1e9,
+                             "recon_per_s": args.steps / s16,
+                             "rel_rmse_vs_fp32_storage": err16},
+            "plain_fp32_eager": {"value": units * args.steps / sp / 1e9,
+                                 "recon_per_s": args.steps / sp},
+        }
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        v, cores, sample, _ = cpu_baseline(c, truth[0, 0].double().cpu().numpy(),
+                                           views_per_step=2, steps=1)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": workload_name(c), "parallelism": f"replicas x{ws}",
+                   "sampler": args.sampler, "graph": "one CUDA graph per reconstruction",
+                   "l2": "working set > L2 (volume, 4 dual volumes, sinograms ~0.5 GB)",
+                   "inputs": "seeded ellipsoid phantom, Poisson noise"},
+        "recon_per_s": recon_s,
+        "samples_per_recon": units,
+        "per_iteration_ms": {"forward": t_fp, "backward": t_bp, "updates": t_up},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "traffic": None,
+                     "kernel": "forward projector (staging + ray kernel)",
+                     "algorithmic_bytes_per_launch": fp_bytes,
+                     "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": P * 4,
+                "d2h_bytes_per_step": V * 4},
+        "gpu_launches": launches * args.steps,
+    }
+    line.update(extra)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--sampler", choices=["soft", "tex"], default="soft")
+    ap.add_argument("--small", action="store_true", help="64^3 smoke-size workload")
+    ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and not args.small:
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,159 @@
+// Voxel-driven FDK-weighted backprojector: every view in one launch, each
+// voxel accumulated in registers and written once.
+//
+// Follows Standard/plug/kernel/backwardKernel.cu:22-53 (+ helper_geometry.h:
+// 26-42) and Beijing/plug/kernel/backwardKernel.cu:18-45: per voxel and view,
+// the detector coordinate of the voxel's projection is sampled bilinearly
+// (border value 0) and weighted by bp_scale * (SDD/L)^power. The reference ran
+// one launch per view (or per 21 views), read-modify-writing the whole volume
+// each time (backwardKernel.cu:50,101-103). Here the view loop is inside the
+// kernel; the projective map of each view (FP64-derived, see geometry.cu)
+// gives the detector coordinates with one reciprocal per voxel-view.
+#include <algorithm>
+#include <string.h>
+
+#include "common.cuh"
+
+namespace dtv {
+
+struct BPParams {
+  int nx, ny, nz, nu, nv, n_views;
+  int power;
+  int extent;
+  float scale;
+  int64_t sino_pad_elems;  // one padded view
+};
+
+constexpr int kBPTile = 16;  // columns per block edge
+constexpr int kZC = 8;       // voxels per thread along z
+constexpr int kBPThreads = kBPTile * kBPTile;
+
+struct SoftBil {
+  const float* s;  // padded view
+  int pu;
+  float mu, mv;
+  __device__ __forceinline__ float operator()(float u, float v) const {
+    const float fu = floorf(u), fv = floorf(v);
+    const float au = u - fu, av = v - fv;
+    const int iu = (int)fminf(fmaxf(fu, -2.f), mu) + kPad;
+    const int iv = (int)fminf(fmaxf(fv, -2.f), mv) + kPad;
+    const float* b = s + iv * pu + iu;
+    const float v00 = __ldg(b), v01 = __ldg(b + 1), v10 = __ldg(b + pu), v11 = __ldg(b + pu + 1);
+    const float c0 = fmaf(au, v01 - v00, v00), c1 = fmaf(au, v11 - v10, v10);
+    return fmaf(av, c1 - c0, c0);
+  }
+};
+
+template <bool kTex>
+__global__ void __launch_bounds__(kBPThreads) bp_kernel(BPParams bp, const BPView* __restrict__ views,
+                                                        const float* __restrict__ spad,
+                                                        cudaTextureObject_t tex,
+                                                        float* __restrict__ out, int accumulate) {
+  const int tiles_x = (bp.nx + kBPTile - 1) / kBPTile;
+  const int i = (blockIdx.x % tiles_x) * kBPTile + (threadIdx.x & 15);
+  const int j = (blockIdx.x / tiles_x) * kBPTile + (threadIdx.x >> 4);
+  const int k0 = blockIdx.y * kZC;
+  if (i >= bp.nx || j >= bp.ny) return;
+  float acc[kZC];
+#pragma unroll
+  for (int z = 0; z < kZC; ++z) acc[z] = 0.f;
+  const float fi = (float)i, fj = (float)j;
+  const int pu = bp.nu + 2 * kPad;
+  const float mu = (float)bp.nu, mv = (float)bp.nv;
+  for (int n = 0; n < bp.n_views; ++n) {
+    const BPView& w = views[n];
+    const float m0 = __ldg(&w.m[0]), m1 = __ldg(&w.m[1]), m2 = __ldg(&w.m[2]), m3 = __ldg(&w.m[3]);
+    const float m4 = __ldg(&w.m[4]), m5 = __ldg(&w.m[5]), m6 = __ldg(&w.m[6]), m7 = __ldg(&w.m[7]);
+    const float m8 = __ldg(&w.m[8]), m9 = __ldg(&w.m[9]), m10 = __ldg(&w.m[10]),
+                m11 = __ldg(&w.m[11]);
+    const float bu = fmaf(m0, fi, fmaf(m1, fj, m3));
+    const float bv = fmaf(m4, fi, fmaf(m5, fj, m7));
+    const float bh = fmaf(m8, fi, fmaf(m9, fj, m11));
+    SoftBil smp{spad + (int64_t)n * bp.sino_pad_elems, pu, mu, mv};
+#pragma unroll
+    for (int z = 0; z < kZC; ++z) {
+      const float fk = (float)(k0 + z);
+      const float h = fmaf(m10, fk, bh);
+      const float rh = __frcp_rn(h);
+      const float u = fmaf(m2, fk, bu) * rh;
+      const float v = fmaf(m6, fk, bv) * rh;
+      float wgt = bp.scale;
+      if (bp.power == 2) wgt *= rh * rh;
+      else if (bp.power == 1) wgt *= rh;
+      if (bp.extent) {
+        const float tx = u + 0.5f, ty = v + 0.5f;
+        if (tx < -1.f || tx > bp.nx + 1.f || ty < -1.f || ty > bp.ny + 1.f) wgt = 0.f;
+      }
+      float val;
+      if constexpr (kTex) val = tex2DLayered<float>(tex, u + 0.5f, v + 0.5f, n);
+      else val = smp(u, v);
+      acc[z] = fmaf(val, wgt, acc[z]);
+    }
+  }
+  const int64_t plane = (int64_t)bp.nx * bp.ny;
+  float* o = out + (int64_t)j * bp.nx + i;
+#pragma unroll
+  for (int z = 0; z < kZC; ++z) {
+    const int k = k0 + z;
+    if (k < bp.nz) {
+      if (accumulate) o[k * plane] += acc[z];
+      else o[k * plane] = acc[z];
+    }
+  }
+}
+
+__global__ void stage_sino_pad_kernel(const float* __restrict__ in, float* __restrict__ out, int nu,
+                                      int nv, int64_t n_views_total) {
+  const int pu = nu + 2 * kPad;
+  const int64_t per = (int64_t)nu * nv, pper = (int64_t)pu * (nv + 2 * kPad);
+  const int64_t total = per * n_views_total;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t n = i / per;
+    const int r = (int)(i - n * per);
+    const int u = r % nu, v = r / nu;
+    out[n * pper + (int64_t)(v + kPad) * pu + u + kPad] = __ldg(in + i);
+  }
+}
+
+int backward_impl(Plan* p, const float* sino, int batch, float* out, int accumulate,
+                  cudaStream_t st) {
+  const GeomParams& gp = p->gp;
+  BPParams bp;
+  bp.nx = gp.nx; bp.ny = gp.ny; bp.nz = gp.nz;
+  bp.nu = gp.nu; bp.nv = gp.nv; bp.n_views = gp.n_views;
+  bp.power = gp.bp_power;
+  bp.extent = gp.bp_extent;
+  bp.scale = (float)gp.bp_scale;
+  bp.sino_pad_elems = (int64_t)(gp.nu + 2 * kPad) * (gp.nv + 2 * kPad);
+  const bool tex = (p->flags & DTV_PLAN_TEX) != 0 && p->sino_tex != nullptr;
+  const int tiles = ((gp.nx + kBPTile - 1) / kBPTile) * ((gp.ny + kBPTile - 1) / kBPTile);
+  dim3 grid(tiles, (gp.nz + kZC - 1) / kZC);
+  const int64_t per_item = (int64_t)gp.nu * gp.nv * gp.n_views;
+  for (int b = 0; b < batch; ++b) {
+    if (tex) {
+      cudaMemcpy3DParms cp;
+      memset(&cp, 0, sizeof(cp));
+      cp.srcPtr = make_cudaPitchedPtr((void*)(sino + b * per_item), gp.nu * sizeof(float), gp.nu,
+                                      gp.nv);
+      cp.dstArray = p->sino_arrays[0];
+      cp.extent = make_cudaExtent(gp.nu, gp.nv, gp.n_views);
+      cp.kind = cudaMemcpyDeviceToDevice;
+      DTV_CUDA_TRY(cudaMemcpy3DAsync(&cp, st));
+      bp_kernel<true><<<grid, kBPThreads, 0, st>>>(bp, p->d_bpv, nullptr, p->sino_tex[0],
+                                                   out + (int64_t)b * gp.nx * gp.ny * gp.nz,
+                                                   accumulate); note_launch();
+    } else {
+      stage_sino_pad_kernel<<<(int)std::min<int64_t>((per_item + 255) / 256, 148 * 16), 256, 0,
+                              st>>>(sino + b * per_item, p->d_sino_pad, gp.nu, gp.nv, gp.n_views); note_launch();
+      DTV_LAUNCH_CHECK();
+      bp_kernel<false><<<grid, kBPThreads, 0, st>>>(bp, p->d_bpv, p->d_sino_pad, 0,
+                                                    out + (int64_t)b * gp.nx * gp.ny * gp.nz,
+                                                    accumulate); note_launch();
+    }
+    DTV_LAUNCH_CHECK();
+  }
+  return DTV_OK;
+}
+
+}  // namespace dtv

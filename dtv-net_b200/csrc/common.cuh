@@ -1,0 +1,139 @@
+// Internal definitions shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "dtv_b200.h"
+
+namespace dtv {
+
+// ---- error reporting -------------------------------------------------------------
+// Host-side count of kernel launches issued by the library (dtv_launch_count).
+void note_launch();
+void set_error(const char* fmt, ...);
+int fail(int code, const char* fmt, ...);
+
+#define DTV_CUDA_TRY(expr)                                                             \
+  do {                                                                                 \
+    cudaError_t _e = (expr);                                                           \
+    if (_e != cudaSuccess)                                                             \
+      return ::dtv::fail(DTV_ERR_CUDA, "%s failed: %s (%s:%d)", #expr,                 \
+                         cudaGetErrorString(_e), __FILE__, __LINE__);                  \
+  } while (0)
+
+#define DTV_CHECK(cond, ...)                                                           \
+  do {                                                                                 \
+    if (!(cond)) return ::dtv::fail(DTV_ERR_INVALID, __VA_ARGS__);                     \
+  } while (0)
+
+// Launch-error check right after a kernel launch.
+#define DTV_LAUNCH_CHECK()                                                             \
+  do {                                                                                 \
+    cudaError_t _e = cudaGetLastError();                                               \
+    if (_e != cudaSuccess)                                                             \
+      return ::dtv::fail(DTV_ERR_CUDA, "kernel launch failed: %s (%s:%d)",             \
+                         cudaGetErrorString(_e), __FILE__, __LINE__);                  \
+  } while (0)
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// ---- storage types -------------------------------------------------------------------
+__device__ __forceinline__ float load_as_float(const float* p, int64_t i) { return __ldg(p + i); }
+__device__ __forceinline__ float load_as_float(const __half* p, int64_t i) {
+  return __half2float(p[i]);
+}
+__device__ __forceinline__ float load_as_float(const __nv_bfloat16* p, int64_t i) {
+  return __bfloat162float(p[i]);
+}
+__device__ __forceinline__ void store_from_float(float* p, int64_t i, float v) { p[i] = v; }
+__device__ __forceinline__ void store_from_float(__half* p, int64_t i, float v) {
+  p[i] = __float2half_rn(v);
+}
+__device__ __forceinline__ void store_from_float(__nv_bfloat16* p, int64_t i, float v) {
+  p[i] = __float2bfloat16_rn(v);
+}
+
+inline int dtype_size(int dt) { return dt == DTV_F32 ? 4 : 2; }
+inline bool dtype_ok(int dt) { return dt == DTV_F32 || dt == DTV_F16 || dt == DTV_BF16; }
+
+// ---- per-view tables (built in FP64 on the host) ------------------------------------
+// Forward projector, index space (voxel (i,j,k) centred at (i,j,k)):
+//   ray to pixel (u,v): r = d0ms + u*U + v*V   (d0ms = pixel(0,0) centre - source)
+//   source S (index) and Sw (world) for the phase rule.
+struct FPView {
+  double s[3];     // source, index coordinates
+  double sw[3];    // source, world coordinates
+  double d0ms[3];  // pixel (0,0) centre minus source, index coordinates
+  double u[3];     // one pixel step along u, index coordinates
+  double v[3];     // one pixel step along v, index coordinates
+  double pad;
+};
+static_assert(sizeof(FPView) == 128, "FPView layout");
+
+// Backprojector: projective map from voxel index (i,j,k,1):
+//   h = m[8..11].x, u = m[0..3].x / h, v = m[4..7].x / h (pixel-index coordinates),
+//   weight = bp_scale * h^-power, with h = L / SDD (distances along the normal).
+struct BPView {
+  float m[12];
+  float pad[4];
+};
+static_assert(sizeof(BPView) == 64, "BPView layout");
+
+struct GeomParams {
+  int nx, ny, nz, nu, nv, n_views;
+  int phase;
+  int bp_power;
+  int bp_extent;
+  double voxel[3];
+  double vol_offset[3];
+  double det_offset[2];
+  double step, scale, bp_scale;
+};
+
+// Host helpers (geometry.cu)
+int build_tables(const dtv_geometry* g, GeomParams* gp, FPView* fpv, BPView* bpv);
+int validate_geometry(const dtv_geometry* g);
+double count_fp_samples(const GeomParams& gp, const FPView* fpv);
+
+// ---- plans -----------------------------------------------------------------------------
+struct Plan {
+  int device;
+  int flags;
+  int max_batch;
+  GeomParams gp;
+  FPView* d_fpv;  // device
+  BPView* d_bpv;  // device
+  // soft sampler staging: zero-padded volumes (border kPad) of max_batch items
+  void* d_vol_pad;
+  int stage_dtype;    // DTV_F32 or DTV_F16
+  int64_t pad_elems;  // elements of one padded volume
+  // soft bilinear staging: zero-padded sinogram of one batch item
+  float* d_sino_pad;
+  // adjoint accumulator: one padded FP32 volume
+  float* d_adj_pad;
+  // texture sampler (DTV_PLAN_TEX): one 3-D array per batch item for the
+  // volume, one layered array for a sinogram
+  cudaArray_t* vol_arrays;
+  cudaTextureObject_t* vol_tex;      // host copy
+  cudaTextureObject_t* vol_tex_dev;  // device copy (kernel argument)
+  cudaSurfaceObject_t* vol_surf;     // staging writes into vol_arrays
+  cudaArray_t* sino_arrays;
+  cudaTextureObject_t* sino_tex;
+  double fp_samples;  // per volume, < 0 until computed
+};
+
+constexpr int kPad = 2;  // zero border of the staged volume
+
+// kernels entry points used across units
+int forward_impl(Plan* p, const void* vol, int vol_dtype, int batch, float* out, int epilogue,
+                 const float* g, float sigma, double* abs_sum, cudaStream_t st);
+int backward_impl(Plan* p, const float* sino, int batch, float* out, int accumulate,
+                  cudaStream_t st);
+int adjoint_impl(Plan* p, const float* sino, int batch, float* out, cudaStream_t st);
+
+}  // namespace dtv

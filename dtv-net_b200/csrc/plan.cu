@@ -1,0 +1,312 @@
+// Plans (device tables + sampler staging) and the projector entry points.
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace dtv {
+
+namespace {
+
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = false;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) == cudaSuccess && cudaSetDevice(dev) == cudaSuccess) ok = true;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+void free_plan(Plan* p) {
+  if (!p) return;
+  if (p->vol_tex) {
+    for (int b = 0; b < p->max_batch; ++b)
+      if (p->vol_tex[b]) cudaDestroyTextureObject(p->vol_tex[b]);
+  }
+  if (p->vol_surf) {
+    for (int b = 0; b < p->max_batch; ++b)
+      if (p->vol_surf[b]) cudaDestroySurfaceObject(p->vol_surf[b]);
+  }
+  free(p->vol_surf);
+  if (p->vol_arrays) {
+    for (int b = 0; b < p->max_batch; ++b)
+      if (p->vol_arrays[b]) cudaFreeArray(p->vol_arrays[b]);
+  }
+  if (p->sino_tex && p->sino_tex[0]) cudaDestroyTextureObject(p->sino_tex[0]);
+  if (p->sino_arrays && p->sino_arrays[0]) cudaFreeArray(p->sino_arrays[0]);
+  free(p->vol_tex);
+  free(p->vol_arrays);
+  free(p->sino_tex);
+  free(p->sino_arrays);
+  cudaFree(p->vol_tex_dev);
+  cudaFree(p->d_fpv);
+  cudaFree(p->d_bpv);
+  cudaFree(p->d_vol_pad);
+  cudaFree(p->d_sino_pad);
+  cudaFree(p->d_adj_pad);
+  delete p;
+}
+
+int make_tex3d(cudaArray_t arr, int filter_linear, cudaTextureObject_t* out) {
+  cudaResourceDesc rd;
+  memset(&rd, 0, sizeof(rd));
+  rd.resType = cudaResourceTypeArray;
+  rd.res.array.array = arr;
+  cudaTextureDesc td;
+  memset(&td, 0, sizeof(td));
+  // same sampling state as the reference (forwardKernel.cu:102-107)
+  td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
+  td.filterMode = filter_linear ? cudaFilterModeLinear : cudaFilterModePoint;
+  td.readMode = cudaReadModeElementType;
+  td.normalizedCoords = 0;
+  DTV_CUDA_TRY(cudaCreateTextureObject(out, &rd, &td, nullptr));
+  return DTV_OK;
+}
+
+int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Plan** out) {
+  DTV_CHECK(out != nullptr, "out is NULL");
+  *out = nullptr;
+  DTV_CHECK(max_batch > 0, "max_batch must be positive");
+  DTV_CHECK((flags & ~(DTV_PLAN_TEX | DTV_PLAN_STAGE_F16)) == 0, "unknown plan flags 0x%x", flags);
+  int ndev = 0;
+  DTV_CUDA_TRY(cudaGetDeviceCount(&ndev));
+  DTV_CHECK(device >= 0 && device < ndev, "device %d out of range (%d devices)", device, ndev);
+  DeviceGuard dg(device);
+  if (!dg.ok) return fail(DTV_ERR_CUDA, "cannot select device %d", device);
+
+  Plan* p = new Plan();
+  memset(p, 0, sizeof(*p));
+  p->device = device;
+  p->flags = flags;
+  p->max_batch = max_batch;
+  p->fp_samples = -1.0;
+  std::vector<FPView> fpv(g ? g->n_views : 0);
+  std::vector<BPView> bpv(g ? g->n_views : 0);
+  int rc = validate_geometry(g);
+  if (rc) {
+    delete p;
+    return rc;
+  }
+  rc = build_tables(g, &p->gp, fpv.data(), bpv.data());
+  if (rc) {
+    delete p;
+    return rc;
+  }
+  const GeomParams& gp = p->gp;
+#define PLAN_CUDA(expr)                                                                  \
+  do {                                                                                   \
+    cudaError_t _e = (expr);                                                             \
+    if (_e != cudaSuccess) {                                                             \
+      free_plan(p);                                                                      \
+      return fail(_e == cudaErrorMemoryAllocation ? DTV_ERR_ALLOC : DTV_ERR_CUDA,        \
+                  "%s failed: %s", #expr, cudaGetErrorString(_e));                       \
+    }                                                                                    \
+  } while (0)
+  PLAN_CUDA(cudaMalloc(&p->d_fpv, sizeof(FPView) * gp.n_views));
+  PLAN_CUDA(cudaMalloc(&p->d_bpv, sizeof(BPView) * gp.n_views));
+  PLAN_CUDA(cudaMemcpy(p->d_fpv, fpv.data(), sizeof(FPView) * gp.n_views, cudaMemcpyHostToDevice));
+  PLAN_CUDA(cudaMemcpy(p->d_bpv, bpv.data(), sizeof(BPView) * gp.n_views, cudaMemcpyHostToDevice));
+
+  p->stage_dtype = (flags & DTV_PLAN_STAGE_F16) ? DTV_F16 : DTV_F32;
+  p->pad_elems = (int64_t)(gp.nx + 2 * kPad) * (gp.ny + 2 * kPad) * (gp.nz + 2 * kPad);
+  const size_t esz = p->stage_dtype == DTV_F16 ? 2 : 4;
+  // Staged volumes: zero border written once here, interiors by each call.
+  PLAN_CUDA(cudaMalloc(&p->d_vol_pad, esz * p->pad_elems * max_batch));
+  PLAN_CUDA(cudaMemset(p->d_vol_pad, 0, esz * p->pad_elems * max_batch));
+  const int64_t sino_pad = (int64_t)(gp.nu + 2 * kPad) * (gp.nv + 2 * kPad) * gp.n_views;
+  PLAN_CUDA(cudaMalloc(&p->d_sino_pad, sizeof(float) * sino_pad));
+  PLAN_CUDA(cudaMemset(p->d_sino_pad, 0, sizeof(float) * sino_pad));
+  PLAN_CUDA(cudaMalloc(&p->d_adj_pad, sizeof(float) * p->pad_elems));
+
+  if (flags & DTV_PLAN_TEX) {
+    p->vol_arrays = (cudaArray_t*)calloc(max_batch, sizeof(cudaArray_t));
+    p->vol_tex = (cudaTextureObject_t*)calloc(max_batch, sizeof(cudaTextureObject_t));
+    p->vol_surf = (cudaSurfaceObject_t*)calloc(max_batch, sizeof(cudaSurfaceObject_t));
+    p->sino_arrays = (cudaArray_t*)calloc(1, sizeof(cudaArray_t));
+    p->sino_tex = (cudaTextureObject_t*)calloc(1, sizeof(cudaTextureObject_t));
+    if (!p->vol_arrays || !p->vol_tex || !p->vol_surf || !p->sino_arrays || !p->sino_tex) {
+      free_plan(p);
+      return fail(DTV_ERR_ALLOC, "host allocation failed");
+    }
+    cudaChannelFormatDesc cd = p->stage_dtype == DTV_F16 ? cudaCreateChannelDescHalf()
+                                                         : cudaCreateChannelDesc<float>();
+    for (int b = 0; b < max_batch; ++b) {
+      PLAN_CUDA(cudaMalloc3DArray(&p->vol_arrays[b], &cd, make_cudaExtent(gp.nx, gp.ny, gp.nz),
+                                  cudaArraySurfaceLoadStore));
+      rc = make_tex3d(p->vol_arrays[b], 1, &p->vol_tex[b]);
+      if (rc) {
+        free_plan(p);
+        return rc;
+      }
+      cudaResourceDesc rd;
+      memset(&rd, 0, sizeof(rd));
+      rd.resType = cudaResourceTypeArray;
+      rd.res.array.array = p->vol_arrays[b];
+      PLAN_CUDA(cudaCreateSurfaceObject(&p->vol_surf[b], &rd));
+    }
+    PLAN_CUDA(cudaMalloc(&p->vol_tex_dev, sizeof(cudaTextureObject_t) * max_batch));
+    PLAN_CUDA(cudaMemcpy(p->vol_tex_dev, p->vol_tex, sizeof(cudaTextureObject_t) * max_batch,
+                         cudaMemcpyHostToDevice));
+    int max_layers = 0;
+    PLAN_CUDA(cudaDeviceGetAttribute(&max_layers, cudaDevAttrMaxTexture2DLayeredLayers, device));
+    if (gp.n_views <= max_layers) {
+      cudaChannelFormatDesc sd = cudaCreateChannelDesc<float>();
+      PLAN_CUDA(cudaMalloc3DArray(&p->sino_arrays[0], &sd,
+                                  make_cudaExtent(gp.nu, gp.nv, gp.n_views), cudaArrayLayered));
+      rc = make_tex3d(p->sino_arrays[0], 1, &p->sino_tex[0]);
+      if (rc) {
+        free_plan(p);
+        return rc;
+      }
+    } else {
+      // more views than layers: the backprojector samples in software
+      free(p->sino_tex);
+      p->sino_tex = nullptr;
+    }
+  }
+#undef PLAN_CUDA
+  *out = p;
+  return DTV_OK;
+}
+
+int check_plan_call(const dtv_plan* plan, int batch) {
+  DTV_CHECK(plan != nullptr, "plan is NULL");
+  const Plan* p = reinterpret_cast<const Plan*>(plan);
+  DTV_CHECK(batch > 0 && batch <= p->max_batch, "batch %d outside [1, %d]", batch, p->max_batch);
+  return DTV_OK;
+}
+
+}  // namespace
+}  // namespace dtv
+
+using namespace dtv;
+
+extern "C" {
+
+int dtv_plan_create(const dtv_geometry* g, int32_t max_batch, int32_t flags, int32_t device,
+                    dtv_plan** out) {
+  Plan* p = nullptr;
+  int rc = create_plan(g, max_batch, flags, device, &p);
+  if (out) *out = reinterpret_cast<dtv_plan*>(p);
+  return rc;
+}
+
+int dtv_plan_destroy(dtv_plan* plan) {
+  if (!plan) return DTV_OK;
+  Plan* p = reinterpret_cast<Plan*>(plan);
+  DeviceGuard dg(p->device);
+  free_plan(p);
+  return DTV_OK;
+}
+
+int dtv_plan_fp_samples(const dtv_plan* plan, double* samples) {
+  DTV_CHECK(plan && samples, "NULL argument");
+  Plan* p = const_cast<Plan*>(reinterpret_cast<const Plan*>(plan));
+  if (p->fp_samples < 0) {
+    std::vector<FPView> fpv(p->gp.n_views);
+    DTV_CUDA_TRY(cudaMemcpy(fpv.data(), p->d_fpv, sizeof(FPView) * p->gp.n_views,
+                            cudaMemcpyDeviceToHost));
+    p->fp_samples = count_fp_samples(p->gp, fpv.data());
+  }
+  *samples = p->fp_samples;
+  return DTV_OK;
+}
+
+int dtv_forward(dtv_plan* plan, const void* vol, int32_t vol_dtype, int32_t batch, float* out,
+                int32_t epilogue, const float* g, float sigma, double* abs_sum, void* stream) {
+  int rc = check_plan_call(plan, batch);
+  if (rc) return rc;
+  DTV_CHECK(vol && out, "NULL volume or output");
+  DTV_CHECK(dtype_ok(vol_dtype), "bad volume dtype %d", vol_dtype);
+  DTV_CHECK(epilogue >= DTV_EPI_STORE && epilogue <= DTV_EPI_PDHG, "bad epilogue %d", epilogue);
+  DTV_CHECK(epilogue == DTV_EPI_STORE || g != nullptr, "epilogue %d needs g", epilogue);
+  Plan* p = reinterpret_cast<Plan*>(plan);
+  DeviceGuard dg(p->device);
+  return forward_impl(p, vol, vol_dtype, batch, out, epilogue, g, sigma, abs_sum, as_stream(stream));
+}
+
+int dtv_backward(dtv_plan* plan, const float* sino, int32_t batch, float* out, int32_t accumulate,
+                 void* stream) {
+  int rc = check_plan_call(plan, batch);
+  if (rc) return rc;
+  DTV_CHECK(sino && out, "NULL sinogram or output");
+  Plan* p = reinterpret_cast<Plan*>(plan);
+  DeviceGuard dg(p->device);
+  return backward_impl(p, sino, batch, out, accumulate, as_stream(stream));
+}
+
+int dtv_backward_adjoint(dtv_plan* plan, const float* sino, int32_t batch, float* out,
+                         void* stream) {
+  int rc = check_plan_call(plan, batch);
+  if (rc) return rc;
+  DTV_CHECK(sino && out, "NULL sinogram or output");
+  Plan* p = reinterpret_cast<Plan*>(plan);
+  DeviceGuard dg(p->device);
+  return adjoint_impl(p, sino, batch, out, as_stream(stream));
+}
+
+static int one_shot(const dtv_geometry* g, int batch, int device, int fwd, const float* in,
+                    float* out, cudaStream_t st) {
+  Plan* p = nullptr;
+  int rc = create_plan(g, batch, 0, device, &p);
+  if (rc) return rc;
+  {
+    DeviceGuard dg(device);
+    rc = fwd ? forward_impl(p, in, DTV_F32, batch, out, DTV_EPI_STORE, nullptr, 0.f, nullptr, st)
+             : backward_impl(p, in, batch, out, 0, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (!rc && e != cudaSuccess) rc = fail(DTV_ERR_CUDA, "sync: %s", cudaGetErrorString(e));
+  }
+  dtv_plan_destroy(reinterpret_cast<dtv_plan*>(p));
+  return rc;
+}
+
+int dtv_standard_forward(const float* volume, int32_t batch, const float* angles_deg,
+                         int32_t n_angles, const int32_t vs[3], const int32_t ds[2], float sid,
+                         float sdd, int32_t device, float* sino, void* stream) {
+  DTV_CHECK(volume && sino, "NULL volume or sinogram");
+  std::vector<double> views(12 * (size_t)(n_angles > 0 ? n_angles : 0));
+  dtv_geometry g;
+  int rc = dtv_geometry_standard(&g, views.data(), angles_deg, n_angles, vs, ds, sid, sdd);
+  if (rc) return rc;
+  return one_shot(&g, batch, device, 1, volume, sino, as_stream(stream));
+}
+
+int dtv_standard_backward(const float* sino, int32_t batch, const float* angles_deg,
+                          int32_t n_angles, const int32_t vs[3], const int32_t ds[2], float sid,
+                          float sdd, int32_t device, float* volume, void* stream) {
+  DTV_CHECK(volume && sino, "NULL volume or sinogram");
+  std::vector<double> views(12 * (size_t)(n_angles > 0 ? n_angles : 0));
+  dtv_geometry g;
+  int rc = dtv_geometry_standard(&g, views.data(), angles_deg, n_angles, vs, ds, sid, sdd);
+  if (rc) return rc;
+  return one_shot(&g, batch, device, 0, sino, volume, as_stream(stream));
+}
+
+int dtv_vector_forward(const float* volume, int32_t batch, const int32_t vs[3],
+                       const int32_t ds[2], const float* pv, int32_t n_views, int32_t device,
+                       float* sino, void* stream) {
+  DTV_CHECK(volume && sino, "NULL volume or sinogram");
+  std::vector<double> views(12 * (size_t)(n_views > 0 ? n_views : 0));
+  dtv_geometry g;
+  int rc = dtv_geometry_vector(&g, views.data(), pv, n_views, vs, ds);
+  if (rc) return rc;
+  return one_shot(&g, batch, device, 1, volume, sino, as_stream(stream));
+}
+
+int dtv_vector_backward(const float* sino, int32_t batch, const int32_t vs[3],
+                        const int32_t ds[2], const float* pv, int32_t n_views, int32_t device,
+                        float* volume, void* stream) {
+  DTV_CHECK(volume && sino, "NULL volume or sinogram");
+  std::vector<double> views(12 * (size_t)(n_views > 0 ? n_views : 0));
+  dtv_geometry g;
+  int rc = dtv_geometry_vector(&g, views.data(), pv, n_views, vs, ds);
+  if (rc) return rc;
+  return one_shot(&g, batch, device, 0, sino, volume, as_stream(stream));
+}
+
+}  // extern "C"

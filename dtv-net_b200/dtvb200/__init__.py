@@ -1,0 +1,23 @@
+"""dtvb200 — B200 cone-beam projector pair and unrolled DTV / FISTA / PDHG updates.
+
+The compute path is the sm_100a kernel library libdtvb200.so behind the C ABI
+of include/dtv_b200.h; this package is its host side. There is no CPU path.
+"""
+from . import _lib
+from ._lib import DtvError
+from .geometry import Geometry, Plan, circular, standard, vector
+from .ops import (BeijingGeometry, Projector, StandardGeometry, StandardGeometryWithFBP,
+                  make_functions)
+from .tv import diff, diff_abs_sums, l1ball
+from .algorithms import ASDPOCS, DTVCP, DTVFISTA, FISTA, power_norm
+
+__all__ = [
+    "DtvError", "Geometry", "Plan", "circular", "standard", "vector", "Projector",
+    "StandardGeometry", "StandardGeometryWithFBP", "BeijingGeometry", "make_functions", "diff",
+    "diff_abs_sums", "l1ball", "DTVCP", "FISTA", "DTVFISTA", "ASDPOCS", "power_norm",
+    "library_path",
+]
+
+
+def library_path() -> str:
+    return _lib.LIB_PATH

@@ -1,0 +1,238 @@
+"""Geometry descriptions and projector plans (host side of the C ABI).
+
+A :class:`Geometry` is the per-view vector form of a cone-beam scan
+(source, detector centre and one-pixel steps U, V per view; FP64). The
+builders reproduce the reference layers' conventions:
+
+* :func:`standard` — model/ConeBeamLayers/Standard (circular orbit; voxel =
+  sample step = sid/sdd, detector pitch 1; forwardKernel.cu:30-40,63,82;
+  backwardKernel.cu:29-50).
+* :func:`vector` — model/ConeBeamLayers/Beijing (per-view [N,12] projection
+  vectors; Beijing/plug/kernel/forwardKernel.cu:24-35, backwardKernel.cu:21-43).
+* :func:`circular` — a circular orbit with explicit voxel size and detector
+  pitch (the general geometry the reference cannot express).
+
+A :class:`Plan` uploads a geometry to one GPU once; its methods run the
+projectors on torch CUDA tensors on the current stream, never synchronising.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import call
+
+_DT = {torch.float32: _lib.DTV_F32, torch.float16: _lib.DTV_F16, torch.bfloat16: _lib.DTV_BF16}
+
+
+@dataclass
+class Geometry:
+    """FP64 per-view geometry plus the scalar conventions of a layer."""
+
+    struct: _lib.dtv_geometry
+    views: np.ndarray  # [n_views, 12] float64, kept alive for struct.views
+
+    @property
+    def volume_size(self):
+        return (self.struct.nx, self.struct.ny, self.struct.nz)
+
+    @property
+    def detector_size(self):
+        return (self.struct.nu, self.struct.nv)
+
+    @property
+    def n_views(self) -> int:
+        return self.struct.n_views
+
+    def vol_shape(self, batch: int = 1):
+        s = self.struct
+        return (batch, 1, s.nz, s.ny, s.nx)
+
+    def sino_shape(self, batch: int = 1):
+        s = self.struct
+        return (batch, 1, s.n_views, s.nv, s.nu)
+
+    def key(self):
+        s = self.struct
+        scal = (s.nx, s.ny, s.nz, s.nu, s.nv, s.n_views, tuple(s.voxel), tuple(s.vol_offset),
+                tuple(s.det_offset), s.fp_step, s.fp_scale, s.fp_phase, s.bp_weight_power,
+                s.bp_scale, s.bp_extent_check)
+        return scal + (self.views.tobytes(),)
+
+
+def _finish(g: _lib.dtv_geometry, views: np.ndarray) -> Geometry:
+    g.views = views.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    return Geometry(g, views)
+
+
+def standard(angles_deg, volume_size, detector_size, sid: float, sdd: float) -> Geometry:
+    """The Standard layer's circular geometry (JITStandardGeometry conventions)."""
+    a = np.ascontiguousarray(np.asarray(angles_deg, dtype=np.float32).ravel())
+    views = np.zeros((a.size, 12), dtype=np.float64)
+    g = _lib.dtv_geometry()
+    call("dtv_geometry_standard", ctypes.byref(g),
+         views.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+         a.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), a.size,
+         _lib.ivec(volume_size), _lib.ivec(detector_size), float(sid), float(sdd))
+    geo = _finish(g, views)
+    geo._angles = a
+    return geo
+
+
+def vector(project_vector, volume_size, detector_size) -> Geometry:
+    """The Beijing layer's per-view vector geometry (JITBeijingGeometry conventions)."""
+    pv = np.ascontiguousarray(np.asarray(project_vector, dtype=np.float32).reshape(-1, 12))
+    views = np.zeros((pv.shape[0], 12), dtype=np.float64)
+    g = _lib.dtv_geometry()
+    call("dtv_geometry_vector", ctypes.byref(g),
+         views.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+         pv.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), pv.shape[0],
+         _lib.ivec(volume_size), _lib.ivec(detector_size))
+    return _finish(g, views)
+
+
+def circular(angles_deg, volume_size, voxel, detector_size, pitch, sod: float,
+             sdd: float) -> Geometry:
+    """Circular orbit with explicit voxel size and detector pitch (centred grids,
+    exact-chord sampling at step = smallest voxel edge)."""
+    a = np.ascontiguousarray(np.asarray(angles_deg, dtype=np.float64).ravel())
+    views = np.zeros((a.size, 12), dtype=np.float64)
+    g = _lib.dtv_geometry()
+    call("dtv_geometry_circular", ctypes.byref(g),
+         views.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+         a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), a.size,
+         _lib.ivec(volume_size), _lib.dvec(voxel), _lib.ivec(detector_size), _lib.dvec(pitch),
+         float(sod), float(sdd))
+    return _finish(g, views)
+
+
+def _stream(device: torch.device) -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def _ptr(t) -> ctypes.c_void_p:
+    return ctypes.c_void_p(0 if t is None else t.data_ptr())
+
+
+def check_input(t: torch.Tensor, name: str, shape=None, dtypes=(torch.float32,)):
+    """The reference's CHECK_INPUT (forwardKernel.cu:15-17) plus shape/dtype."""
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise RuntimeError(f"{name} must be a CUDA tensor")
+    if not t.is_contiguous():
+        raise RuntimeError(f"{name} must be contiguous")
+    if t.dtype not in dtypes:
+        raise RuntimeError(f"{name} must have dtype in {dtypes}, got {t.dtype}")
+    if shape is not None and tuple(t.shape) != tuple(shape):
+        raise RuntimeError(f"{name} must have shape {tuple(shape)}, got {tuple(t.shape)}")
+
+
+class Plan:
+    """A geometry uploaded to one GPU with sampler staging for ``max_batch``
+    volumes. ``sampler``: "soft" (software trilinear, FP32 weights; required
+    for the exact adjoint) or "tex" (hardware texture filtering, like the
+    reference). ``stage_f16`` stages projected volumes as FP16."""
+
+    def __init__(self, geometry: Geometry, max_batch: int = 1, sampler: str = "soft",
+                 stage_f16: bool = False, device=None):
+        if sampler not in ("soft", "tex"):
+            raise ValueError("sampler must be 'soft' or 'tex'")
+        dev = torch.device("cuda", torch.cuda.current_device()) if device is None else \
+            torch.device(device)
+        if dev.type != "cuda":
+            raise RuntimeError("a Plan needs a CUDA device")
+        self.device = torch.device("cuda", dev.index if dev.index is not None
+                                   else torch.cuda.current_device())
+        self.geometry = geometry
+        self.max_batch = int(max_batch)
+        self.sampler = sampler
+        self.stage_f16 = bool(stage_f16)
+        flags = (_lib.DTV_PLAN_TEX if sampler == "tex" else 0) | \
+                (_lib.DTV_PLAN_STAGE_F16 if stage_f16 else 0)
+        h = ctypes.c_void_p()
+        call("dtv_plan_create", ctypes.byref(geometry.struct), self.max_batch, flags,
+             self.device.index, ctypes.byref(h))
+        self._h = h
+
+    # ------------------------------------------------------------------ shapes
+    def vol_shape(self, batch: int = 1):
+        return self.geometry.vol_shape(batch)
+
+    def sino_shape(self, batch: int = 1):
+        return self.geometry.sino_shape(batch)
+
+    def fp_samples(self) -> float:
+        """Forward-projector samples per volume (exact chords / step)."""
+        out = ctypes.c_double()
+        call("dtv_plan_fp_samples", self._h, ctypes.byref(out))
+        return out.value
+
+    def _batch_of(self, t: torch.Tensor, per_item: int) -> int:
+        b = t.numel() // per_item
+        if b * per_item != t.numel() or b < 1:
+            raise RuntimeError(f"tensor of {t.numel()} elements is not a whole batch")
+        if b > self.max_batch:
+            raise RuntimeError(f"batch {b} exceeds the plan's max_batch {self.max_batch}")
+        return b
+
+    # ------------------------------------------------------------------ ops
+    def forward(self, vol: torch.Tensor, out: torch.Tensor = None, epilogue: int = 0,
+                g: torch.Tensor = None, sigma: float = 0.0,
+                abs_sum: torch.Tensor = None) -> torch.Tensor:
+        """Forward projection of [B,1,Z,Y,X] (f32/f16/bf16) -> [B,1,N,H,W] f32.
+        epilogue: DTV_EPI_STORE / DTV_EPI_RESIDUAL (out = FP - g) / DTV_EPI_PDHG
+        (out = (out + sigma*(FP - g))/(1+sigma)). abs_sum (float64, 1 element)
+        accumulates sum|FP - g| (or sum|FP| for STORE)."""
+        check_input(vol, "volume", dtypes=tuple(_DT))
+        per = int(np.prod(self.vol_shape(1)))
+        b = self._batch_of(vol, per)
+        shape = self.sino_shape(b)
+        if out is None:
+            out = torch.empty(shape, device=vol.device, dtype=torch.float32)
+        check_input(out, "out", shape)
+        if g is not None:
+            check_input(g, "g", shape)
+        if abs_sum is not None:
+            check_input(abs_sum, "abs_sum", dtypes=(torch.float64,))
+        call("dtv_forward", self._h, _ptr(vol), _DT[vol.dtype], b, _ptr(out), int(epilogue),
+             _ptr(g), float(sigma), _ptr(abs_sum), _stream(vol.device))
+        return out
+
+    def backward(self, sino: torch.Tensor, out: torch.Tensor = None,
+                 accumulate: bool = False) -> torch.Tensor:
+        """FDK-weighted voxel-driven backprojection [B,1,N,H,W] -> [B,1,Z,Y,X]."""
+        check_input(sino, "sino")
+        b = self._batch_of(sino, int(np.prod(self.sino_shape(1))))
+        shape = self.vol_shape(b)
+        if out is None:
+            out = torch.empty(shape, device=sino.device, dtype=torch.float32)
+            accumulate = False
+        check_input(out, "out", shape)
+        call("dtv_backward", self._h, _ptr(sino), b, _ptr(out), int(bool(accumulate)),
+             _stream(sino.device))
+        return out
+
+    def adjoint(self, sino: torch.Tensor, out: torch.Tensor = None) -> torch.Tensor:
+        """Exact transpose of forward (STORE): A^T sino."""
+        check_input(sino, "sino")
+        b = self._batch_of(sino, int(np.prod(self.sino_shape(1))))
+        shape = self.vol_shape(b)
+        if out is None:
+            out = torch.empty(shape, device=sino.device, dtype=torch.float32)
+        check_input(out, "out", shape)
+        call("dtv_backward_adjoint", self._h, _ptr(sino), b, _ptr(out), _stream(sino.device))
+        return out
+
+    def close(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h is not None and h.value:
+            _lib.load().dtv_plan_destroy(h)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

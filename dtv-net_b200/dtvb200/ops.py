@@ -1,0 +1,178 @@
+"""Projector operators for torch: autograd Functions and the geometry layers.
+
+Mirrors model/ConeBeamLayers/Standard/StandardGeometry.py and
+model/ConeBeamLayers/Beijing/BeijingGeometry.py. Two pairings exist:
+
+* the reference pairing (``matched=False``): ForwardProjection's gradient is
+  the FDK backprojector and BackProjection's gradient is the forward
+  projector, exactly as StandardGeometry.py:10-34 wires them (the FDK
+  backprojector is NOT the transpose of the forward projector);
+* the matched pairing (``matched=True``): the forward projector's gradient is
+  its exact transpose (dtv_backward_adjoint), so unrolled networks get true
+  gradients; checked by the dot-product test.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+from .geometry import Geometry, Plan
+
+
+class Projector:
+    """Plans of one geometry, created lazily per (device, sampler) and grown
+    to the largest batch seen."""
+
+    def __init__(self, geometry: Geometry, sampler: str = "soft", stage_f16: bool = False,
+                 max_batch: int = 1):
+        self.geometry = geometry
+        self.sampler = sampler
+        self.stage_f16 = stage_f16
+        self.max_batch = max_batch
+        self._plans = {}
+
+    def plan(self, device: torch.device, batch: int = 1, sampler: str = None) -> Plan:
+        sampler = sampler or self.sampler
+        key = (device.index, sampler)
+        p = self._plans.get(key)
+        if p is None or p.max_batch < batch:
+            if p is not None:
+                p.close()
+            p = Plan(self.geometry, max(batch, self.max_batch), sampler, self.stage_f16, device)
+            self._plans[key] = p
+        return p
+
+    def batch_of(self, t: torch.Tensor, volume: bool) -> int:
+        per = int(np.prod(self.geometry.vol_shape(1) if volume else self.geometry.sino_shape(1)))
+        return max(1, t.numel() // per)
+
+    def fp(self, x: torch.Tensor) -> torch.Tensor:
+        x = x.contiguous()
+        return self.plan(x.device, self.batch_of(x, True)).forward(x)
+
+    def bp(self, s: torch.Tensor) -> torch.Tensor:
+        s = s.contiguous()
+        return self.plan(s.device, self.batch_of(s, False)).backward(s)
+
+    def adjoint(self, s: torch.Tensor) -> torch.Tensor:
+        s = s.contiguous()
+        return self.plan(s.device, self.batch_of(s, False), sampler="soft").adjoint(s)
+
+    def fp_soft(self, x: torch.Tensor) -> torch.Tensor:
+        x = x.contiguous()
+        return self.plan(x.device, self.batch_of(x, True), sampler="soft").forward(x)
+
+
+def make_functions(projector: Projector, matched: bool = False):
+    """(ForwardProjection, BackProjection) autograd Functions bound to a
+    projector, with the reference pairing or the matched-adjoint pairing."""
+
+    class ForwardProjection(torch.autograd.Function):
+        """StandardGeometry.py:10-21."""
+
+        @staticmethod
+        def forward(ctx, input):
+            if matched:
+                return projector.fp_soft(input)
+            return projector.fp(input)
+
+        @staticmethod
+        def backward(ctx, grad):
+            if matched:
+                return projector.adjoint(grad)
+            return projector.bp(grad)
+
+    class BackProjection(torch.autograd.Function):
+        """StandardGeometry.py:23-34 (matched: the adjoint A^T)."""
+
+        @staticmethod
+        def forward(ctx, input):
+            if matched:
+                return projector.adjoint(input)
+            return projector.bp(input)
+
+        @staticmethod
+        def backward(ctx, grad):
+            if matched:
+                return projector.fp_soft(grad)
+            return projector.fp(grad)
+
+    return ForwardProjection, BackProjection
+
+
+class StandardGeometry(torch.nn.Module):
+    """x - lamb * BP(FP(x) - p)  (StandardGeometry.py:36-43)."""
+
+    def __init__(self, projector: Projector, matched: bool = False, lamb: float = 1.0):
+        super().__init__()
+        self.FP, self.BP = make_functions(projector, matched)
+        self.lamb = lamb
+
+    def forward(self, x, p):
+        residual = self.FP.apply(x) - p
+        return x - self.lamb * self.BP.apply(residual)
+
+
+class BeijingGeometry(torch.nn.Module):
+    """-lamb * BP(FP(x) - p)  (BeijingGeometry.py:41-48)."""
+
+    def __init__(self, projector: Projector, matched: bool = False, lamb: float = 10e-3,
+                 sample_interval: float = 1.0):
+        super().__init__()
+        self.FP, self.BP = make_functions(projector, matched)
+        self.lamb = lamb
+        self.sample_interval = sample_interval
+
+    def forward(self, x, p):
+        residual = self.FP.apply(x) * self.sample_interval - p
+        return -self.lamb * self.BP.apply(residual)
+
+
+def ramp_kernel(width: int) -> torch.Tensor:
+    """Spatial Ram-Lak kernel of width+1 taps: 1/8 at the centre, 0 at even
+    offsets, -1/(2 pi^2 n^2) at odd offsets n (StandardGeometry.py:83-93)."""
+    f = np.ones((1, 1, 1, width + 1), dtype=np.float32)
+    mid = np.floor(width / 2)
+    for i in range(width + 1):
+        if (i - mid) % 2 == 0:
+            f[..., i] = 0
+        else:
+            f[..., i] = -0.5 / (np.pi * np.pi * (i - mid) * (i - mid))
+        if i == mid:
+            f[..., i] = 1 / 8
+    return torch.from_numpy(f)
+
+
+def cos_weight(n_views: int, detector_size, sdd: float) -> torch.Tensor:
+    """sdd / sqrt(sdd^2 + (i-H/2)^2 + (j-W/2)^2) over the detector
+    (StandardGeometry.py:68-74)."""
+    W, H = detector_size
+    i = np.arange(H)[:, None] - H / 2
+    j = np.arange(W)[None, :] - W / 2
+    w = (sdd / np.sqrt(sdd ** 2 + i ** 2 + j ** 2)).astype(np.float32)
+    return torch.from_numpy(np.broadcast_to(w, (1, 1, n_views, H, W)).copy())
+
+
+class StandardGeometryWithFBP(torch.nn.Module):
+    """lamb * BP(ramp * (cos * (FP(x) - p)))  (StandardGeometry.py:45-66)."""
+
+    def __init__(self, projector: Projector, sdd: float, matched: bool = False):
+        super().__init__()
+        g = projector.geometry
+        self.FP, self.BP = make_functions(projector, matched)
+        self.lamb = torch.nn.Parameter(torch.tensor(1.0), requires_grad=False)
+        self.cosWeight = torch.nn.Parameter(cos_weight(g.n_views, g.detector_size, sdd),
+                                            requires_grad=False)
+        self.ramp = torch.nn.Parameter(ramp_kernel(g.detector_size[0]), requires_grad=False)
+        self.width = g.detector_size[0]
+
+    def forward(self, x, p):
+        residual = self.FP.apply(x) - p
+        residual = residual * self.cosWeight
+        b, c, a, h, w = residual.size()
+        residual = residual.view(b, c, a * h, w)
+        residual = torch.nn.functional.conv2d(residual, self.ramp, stride=1,
+                                              padding=(0, int(self.width / 2)))
+        residual = residual.view(b, c, a, h, w)
+        return self.lamb * self.BP.apply(residual.contiguous())

@@ -1,0 +1,298 @@
+"""GPU parity tests of the projector kernels through the C ABI: against the
+FP64 oracle (same geometry), against the reference CUDA kernels' golden
+outputs, the dot-product adjoint test, precision modes, epilogues, batching,
+edge cases and the drop-in modules."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import dtvb200
+import oracle as O
+from dtvb200 import _lib
+from helpers import blob_volume, rel_max, rel_rmse, vector_views
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def make_case(kind):
+    """(library geometry, oracle geometry) pairs covering every phase rule."""
+    if kind == "standard":
+        ang = np.linspace(0, 360, 12, endpoint=False).astype(np.float32)
+        vs, ds = (24, 20, 10), (33, 17)
+        return (dtvb200.standard(ang, vs, ds, 500.0, 1000.0),
+                O.standard_geometry(ang.astype(np.float64), vs, ds, 500.0, 1000.0))
+    if kind == "standard_odd":
+        ang = np.linspace(0, 360, 7, endpoint=False).astype(np.float32)
+        vs, ds = (17, 23, 9), (29, 13)
+        return (dtvb200.standard(ang, vs, ds, 300.0, 800.0),
+                O.standard_geometry(ang.astype(np.float64), vs, ds, 300.0, 800.0))
+    if kind == "vector":
+        pv = vector_views(42, 40.0, 70.0, 1.6, 1.7, 1.5)
+        vs, ds = (16, 14, 10), (20, 12)
+        return dtvb200.vector(pv, vs, ds), O.vector_geometry(pv, vs, ds)
+    if kind == "box":
+        ang = np.linspace(0, 360, 10, endpoint=False)
+        vs, ds, vox, pitch = (20, 18, 12), (28, 20), (1.0, 0.9, 1.2), (1.2, 1.1)
+        return (dtvb200.circular(ang, vs, vox, ds, pitch, 500, 1000),
+                O.circular_geometry(ang, vs, vox, ds, pitch, 500, 1000))
+    raise ValueError(kind)
+
+
+KINDS = ["standard", "standard_odd", "vector", "box"]
+
+
+def to_dev(a, dev, dtype=torch.float32):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(dev, dtype)
+
+
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("batch", [1, 2])
+def test_forward_soft_matches_oracle(cuda, kind, batch):
+    g, og = make_case(kind)
+    plan = dtvb200.Plan(g, max_batch=2, device=cuda)
+    rng = np.random.default_rng(10)
+    vol = blob_volume(rng, og.vol_shape, batch)
+    out = plan.forward(to_dev(vol, cuda)).cpu().numpy()
+    ref = O.forward(og, vol).reshape(out.shape)
+    # FP32 ray sums against FP64: tolerance 1e-5 relative RMSE, 1e-4 relative max
+    assert rel_rmse(out, ref) < 1e-5
+    assert rel_max(out, ref) < 1e-4
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_forward_tex_matches_oracle_tex_mode(cuda, kind):
+    g, og = make_case(kind)
+    plan = dtvb200.Plan(g, max_batch=1, sampler="tex", device=cuda)
+    vol = blob_volume(np.random.default_rng(11), og.vol_shape, 1)
+    out = plan.forward(to_dev(vol, cuda)).cpu().numpy()
+    refq = O.forward(og, vol, q=True).reshape(out.shape)
+    ref = O.forward(og, vol).reshape(out.shape)
+    # hardware filtering keeps 8 fractional weight bits
+    assert rel_rmse(out, refq) < 5e-4
+    assert rel_rmse(out, ref) < 5e-3
+
+
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("sampler", ["soft", "tex"])
+def test_backward_fdk_matches_oracle(cuda, kind, sampler):
+    g, og = make_case(kind)
+    plan = dtvb200.Plan(g, max_batch=2, sampler=sampler, device=cuda)
+    rng = np.random.default_rng(12)
+    sino = rng.random((2, 1) + og.sino_shape).astype(np.float32)
+    out = plan.backward(to_dev(sino, cuda)).cpu().numpy()
+    if sampler == "soft":
+        ref = O.backward(og, sino).reshape(out.shape)
+        assert rel_rmse(out, ref) < 1e-5
+        assert rel_max(out, ref) < 1e-4
+    else:
+        ref = O.backward(og, sino, q=True).reshape(out.shape)
+        assert rel_rmse(out, ref) < 5e-4
+
+
+def test_backward_accumulate(cuda):
+    g, og = make_case("standard")
+    plan = dtvb200.Plan(g, device=cuda)
+    sino = to_dev(np.random.default_rng(13).random((1, 1) + og.sino_shape), cuda)
+    a = plan.backward(sino)
+    b = a.clone()
+    plan.backward(sino, out=b, accumulate=True)
+    assert torch.allclose(b, 2 * a, rtol=1e-6, atol=0)
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_adjoint_matches_oracle_and_dot_test(cuda, kind):
+    g, og = make_case(kind)
+    plan = dtvb200.Plan(g, max_batch=2, device=cuda)
+    rng = np.random.default_rng(14)
+    y = rng.random((2, 1) + og.sino_shape).astype(np.float32)
+    x = rng.random((2, 1) + og.vol_shape).astype(np.float32)
+    aty = plan.adjoint(to_dev(y, cuda)).cpu().numpy()
+    ref = O.adjoint(og, y).reshape(aty.shape)
+    assert rel_rmse(aty, ref) < 1e-5
+    ax = plan.forward(to_dev(x, cuda)).cpu().numpy()
+    lhs = float((ax.astype(np.float64) * y).sum())
+    rhs = float((x.astype(np.float64) * aty).sum())
+    # <Ax, y> = <x, A^T y> to 1e-5 relative
+    assert abs(lhs - rhs) / abs(lhs) < 1e-5
+
+
+@pytest.mark.parametrize("vdt", [torch.float16, torch.bfloat16])
+def test_forward_16bit_inputs(cuda, vdt):
+    g, og = make_case("box")
+    plan = dtvb200.Plan(g, device=cuda)
+    vol = blob_volume(np.random.default_rng(15), og.vol_shape, 1)
+    v16 = to_dev(vol, cuda, vdt)
+    out = plan.forward(v16).cpu().numpy()
+    ref = O.forward(og, v16.float().cpu().numpy()).reshape(out.shape)
+    assert rel_rmse(out, ref) < 1e-5  # exact on the rounded input
+    assert rel_rmse(out, O.forward(og, vol).reshape(out.shape)) < (2e-3 if vdt == torch.float16 else 8e-3)
+
+
+def test_forward_stage_f16(cuda):
+    g, og = make_case("standard")
+    plan = dtvb200.Plan(g, stage_f16=True, device=cuda)
+    vol = blob_volume(np.random.default_rng(16), og.vol_shape, 1)
+    out = plan.forward(to_dev(vol, cuda)).cpu().numpy()
+    assert rel_rmse(out, O.forward(og, vol).reshape(out.shape)) < 1e-3
+
+
+def test_forward_epilogues(cuda):
+    g, og = make_case("standard_odd")
+    plan = dtvb200.Plan(g, device=cuda)
+    rng = np.random.default_rng(17)
+    vol = to_dev(blob_volume(rng, og.vol_shape, 1), cuda)
+    gs = to_dev(rng.random((1, 1) + og.sino_shape), cuda)
+    fp = plan.forward(vol)
+    acc = torch.zeros(1, dtype=torch.float64, device=cuda)
+    res = plan.forward(vol, epilogue=_lib.DTV_EPI_RESIDUAL, g=gs, abs_sum=acc)
+    assert torch.allclose(res, fp - gs, atol=1e-6)
+    assert float(acc) == pytest.approx(float((fp - gs).abs().double().sum()), rel=1e-6)
+    w0 = to_dev(rng.random((1, 1) + og.sino_shape), cuda)
+    w = w0.clone()
+    sigma = 0.3
+    plan.forward(vol, out=w, epilogue=_lib.DTV_EPI_PDHG, g=gs, sigma=sigma)
+    assert torch.allclose(w, (w0 + sigma * (fp - gs)) / (1 + sigma), atol=1e-6)
+
+
+def test_rays_missing_the_volume_give_zero(cuda):
+    # detector shifted far off axis: no ray meets the volume
+    ang = np.array([0.0, 90.0], dtype=np.float32)
+    g = dtvb200.standard(ang, (8, 8, 4), (16, 16), 500.0, 1000.0)
+    g.views[:, 5] += 5000.0  # move the detector centres up along z
+    plan = dtvb200.Plan(g, device=cuda)
+    out = plan.forward(torch.ones(g.vol_shape(1), device=cuda))
+    assert float(out.abs().max()) == 0.0
+
+
+def test_determinism(cuda):
+    g, og = make_case("box")
+    plan = dtvb200.Plan(g, device=cuda)
+    rng = np.random.default_rng(18)
+    vol = to_dev(blob_volume(rng, og.vol_shape, 1), cuda)
+    sino = to_dev(rng.random((1, 1) + og.sino_shape), cuda)
+    assert torch.equal(plan.forward(vol), plan.forward(vol))
+    assert torch.equal(plan.backward(sino), plan.backward(sino))
+    a, b = plan.adjoint(sino), plan.adjoint(sino)  # float atomics: order may vary
+    assert rel_max(a.cpu().numpy(), b.cpu().numpy()) < 1e-5
+
+
+def test_input_validation(cuda):
+    g, og = make_case("standard")
+    plan = dtvb200.Plan(g, max_batch=1, device=cuda)
+    vol = torch.zeros(g.vol_shape(1), device=cuda)
+    with pytest.raises(RuntimeError, match="contiguous"):
+        plan.forward(vol.transpose(3, 4))
+    with pytest.raises(RuntimeError, match="max_batch"):
+        plan.forward(torch.zeros(g.vol_shape(2), device=cuda))
+    with pytest.raises(RuntimeError, match="CUDA"):
+        plan.forward(vol.cpu())
+    with pytest.raises(dtvb200.DtvError):
+        plan.forward(vol, epilogue=_lib.DTV_EPI_RESIDUAL)  # needs g
+
+
+def test_fp_samples_match_oracle(cuda):
+    for kind in KINDS:
+        g, og = make_case(kind)
+        plan = dtvb200.Plan(g, device=cuda)
+        assert plan.fp_samples() == O.fp_samples(og)
+
+
+# ----------------------------------------------------------- reference golden outputs
+def _ref_proj():
+    p = os.path.join(GOLDEN, "ref_projectors.npz")
+    if not os.path.exists(p):
+        pytest.skip("ref_projectors.npz not generated yet")
+    return np.load(p)
+
+
+@pytest.mark.parametrize("name", ["s1", "s2", "s3"])
+@pytest.mark.parametrize("sampler", ["soft", "tex"])
+def test_matches_reference_kernels_standard(cuda, name, sampler):
+    """Through the drop-in module with the reference's argument list."""
+    z = _ref_proj()
+    import JITStandardGeometry as J
+    X, Y, Z, W, H, n, b = (int(v) for v in z[f"{name}_sizes"])
+    sid, sdd = (float(v) for v in z[f"{name}_geom"])
+    ang = torch.from_numpy(z[f"{name}_angles"]).to(cuda)
+    vs, ds = torch.tensor([X, Y, Z]).to(cuda), torch.tensor([W, H]).to(cuda)
+    old = J._SAMPLER
+    J._SAMPLER, J._plans = sampler, {}
+    try:
+        fp = J.forward(to_dev(z[f"{name}_vol"], cuda), ang, vs, ds, sid, sdd, 0)
+        bp = J.backward(to_dev(z[f"{name}_sino_in"], cuda), ang, vs, ds, sid, sdd, 0)
+    finally:
+        J._SAMPLER, J._plans = old, {}
+    assert fp.shape == z[f"{name}_fp"].shape and bp.shape == z[f"{name}_bp"].shape
+    tol = 5e-4 if sampler == "tex" else 5e-3  # the reference filters with 1/256 weights
+    assert rel_rmse(fp.cpu().numpy(), z[f"{name}_fp"]) < tol
+    assert rel_rmse(bp.cpu().numpy(), z[f"{name}_bp"]) < tol
+
+
+@pytest.mark.parametrize("sampler", ["soft", "tex"])
+def test_matches_reference_kernels_vector(cuda, sampler):
+    z = _ref_proj()
+    import JITBeijingGeometry as J
+    import JITStandardGeometry as JS
+    X, Y, Z, W, H, n, b = (int(v) for v in z["v_sizes"])
+    vs, ds = torch.IntTensor([X, Y, Z]).to(cuda), torch.IntTensor([W, H]).to(cuda)
+    pv = torch.from_numpy(z["v_pv"]).to(cuda)
+    import JITBeijingGeometry
+    JITBeijingGeometry._SAMPLER, J._plans = sampler, {}
+    try:
+        fp = J.forward(to_dev(z["v_vol"], cuda), vs, ds, pv, 0)
+        bp = J.backward(to_dev(z["v_sino_in"], cuda), vs, ds, pv, 0)
+    finally:
+        JITBeijingGeometry._SAMPLER, J._plans = JS._SAMPLER, {}
+    tol = 5e-4 if sampler == "tex" else 5e-3
+    assert rel_rmse(fp.cpu().numpy(), z["v_fp"]) < tol
+    assert rel_rmse(bp.cpu().numpy(), z["v_bp"]) < tol
+
+
+def test_standard_layers_autograd(cuda):
+    """Reference pairing: grad of FP is the FDK BP (StandardGeometry.py:17-21);
+    matched pairing: grad of FP is the exact adjoint."""
+    g, og = make_case("standard")
+    proj = dtvb200.Projector(g)
+    FP, BP = dtvb200.make_functions(proj, matched=False)
+    x = to_dev(blob_volume(np.random.default_rng(19), og.vol_shape, 1), cuda).requires_grad_()
+    y = FP.apply(x)
+    gy = torch.rand_like(y)
+    y.backward(gy)
+    assert torch.allclose(x.grad, proj.bp(gy), rtol=1e-6, atol=1e-6)
+    FPm, BPm = dtvb200.make_functions(proj, matched=True)
+    x.grad = None
+    FPm.apply(x).backward(gy)
+    assert torch.allclose(x.grad, proj.adjoint(gy), rtol=1e-4, atol=1e-5)
+    layer = dtvb200.StandardGeometry(proj, matched=True)
+    p = torch.rand_like(y)
+    out = layer(x.detach(), p)
+    assert out.shape == x.shape
+
+
+def test_gradcheck_matched_on_random_voxels(cuda):
+    """Finite differences of L(x) = 0.5||Ax - p||^2 on 16 random voxels agree
+    with the autograd gradient through the matched adjoint."""
+    g, og = make_case("box")
+    proj = dtvb200.Projector(g)
+    FP, _ = dtvb200.make_functions(proj, matched=True)
+    rng = np.random.default_rng(20)
+    x = to_dev(blob_volume(rng, og.vol_shape, 1), cuda).double()
+    p = torch.rand(g.sino_shape(1), device=cuda, dtype=torch.float64)
+
+    def loss(xx):
+        return 0.5 * float(((FP.apply(xx.float()).double() - p) ** 2).sum())
+
+    xg = x.float().clone().requires_grad_()
+    (0.5 * ((FP.apply(xg).double() - p) ** 2).sum()).backward()
+    grad = xg.grad.double().flatten()
+    idx = rng.choice(x.numel(), 16, replace=False)
+    h = 1e-2
+    for i in idx:
+        e = torch.zeros_like(x).flatten()
+        e[i] = h
+        e = e.reshape(x.shape)
+        fd = (loss(x + e) - loss(x - e)) / (2 * h)
+        assert abs(fd - float(grad[i])) <= 2e-3 * max(1.0, abs(fd))
