@@ -90,13 +90,17 @@ def test_oracle_pinned_to_reference_standard(name):
     ang = z[f"{name}_angles"].astype(np.float32).astype(np.float64)
     fp = O.forward_standard_literal(z[f"{name}_vol"], ang, (X, Y, Z), (W, H), sid, sdd, q=1)
     bp = O.backward_standard_literal(z[f"{name}_sino_in"], ang, (X, Y, Z), (W, H), sid, sdd, q=1)
-    # texture filtering carries 1/256 weights; the tex-faithful oracle mode
-    # reproduces the reference kernels to single-precision accuracy
-    assert rel_rmse(fp, z[f"{name}_fp"].reshape(fp.shape)) < 2e-4
-    assert rel_rmse(bp, z[f"{name}_bp"].reshape(bp.shape)) < 2e-4
-    # exact weights differ from the reference by the quantisation only
+    # The reference kernels filter with 1/256 texture weights and compute their
+    # coordinates in float32 (sample positions ~1e3 voxels from the origin in the
+    # forward projector, products ~1e6 in the line intersection of the
+    # backprojector). Measured: 1.5e-4 - 4e-4 relative RMSE with quantised
+    # weights, <= 5.3e-4 with exact weights.
+    assert rel_rmse(fp, z[f"{name}_fp"].reshape(fp.shape)) < 6e-4
+    assert rel_rmse(bp, z[f"{name}_bp"].reshape(bp.shape)) < 6e-4
     fpe = O.forward_standard_literal(z[f"{name}_vol"], ang, (X, Y, Z), (W, H), sid, sdd, q=0)
-    assert rel_rmse(fpe, z[f"{name}_fp"].reshape(fp.shape)) < 5e-3
+    bpe = O.backward_standard_literal(z[f"{name}_sino_in"], ang, (X, Y, Z), (W, H), sid, sdd, q=0)
+    assert rel_rmse(fpe, z[f"{name}_fp"].reshape(fp.shape)) < 1e-3
+    assert rel_rmse(bpe, z[f"{name}_bp"].reshape(bp.shape)) < 1e-3
 
 
 def test_oracle_pinned_to_reference_vector():
@@ -105,8 +109,8 @@ def test_oracle_pinned_to_reference_vector():
     pv = z["v_pv"]
     fp = O.forward_vector_literal(z["v_vol"], pv, (X, Y, Z), (W, H), q=1)
     bp = O.backward_vector_literal(z["v_sino_in"], pv, (X, Y, Z), (W, H), q=1)
-    assert rel_rmse(fp, z["v_fp"].reshape(fp.shape)) < 2e-4
-    assert rel_rmse(bp, z["v_bp"].reshape(bp.shape)) < 2e-4
+    assert rel_rmse(fp, z["v_fp"].reshape(fp.shape)) < 6e-4
+    assert rel_rmse(bp, z["v_bp"].reshape(bp.shape)) < 6e-4
 
 
 def _ref_utils():
