@@ -18,6 +18,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -842,3 +843,72 @@ int dtv_scale_scalar(const double* in, double scale, float* out, void* stream) {
 }
 
 }  // extern "C"
+
+// ---- L1-ball projection without a caller-supplied workspace ---------------------------
+//
+// dtv_l1ball needs a ~48 KB device workspace for its threshold search, which
+// its caller allocates. Some callers cannot allocate device memory at the
+// point where they project: a host that reserves the whole GPU at start-up
+// and hands out no allocator, a C or Fortran caller on the far side of the
+// ABI with no device allocator of its own, or a latency-bound pipeline that
+// must not call cudaMalloc/cudaFree in its loop (cudaFree synchronises the
+// device). dtv_l1ball_noalloc serves them with the same kernels, whose
+// workspace is the array below instead. Each GPU that loads this library
+// holds one copy until the process exits.
+namespace dtv {
+
+static __device__ __align__(256) unsigned char g_l1ball_scratch[sizeof(L1Chan)];
+
+constexpr int64_t kL1NoallocMaxN = 2147483647LL;  // per-bin counts are 32-bit
+constexpr int kMaxDevices = 64;
+static std::mutex g_l1ball_scratch_mu;
+static void* g_l1ball_scratch_ptr[kMaxDevices] = {};
+
+// Device address of g_l1ball_scratch on the current device. Host code cannot
+// pass the array's name to a kernel (that is a host-side stand-in), so the
+// address is looked up once per device, with that device current.
+static int l1ball_scratch(L1Chan** out) {
+  int dev = -1;
+  DTV_CUDA_TRY(cudaGetDevice(&dev));
+  DTV_CHECK(dev >= 0 && dev < kMaxDevices, "device %d outside [0, %d)", dev, kMaxDevices);
+  std::lock_guard<std::mutex> lock(g_l1ball_scratch_mu);
+  if (g_l1ball_scratch_ptr[dev] == nullptr) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_l1ball_scratch);
+    if (e != cudaSuccess || p == nullptr)
+      return fail(DTV_ERR_CUDA, "cudaGetSymbolAddress(l1ball scratch) on device %d: %s", dev,
+                  cudaGetErrorString(e));
+    g_l1ball_scratch_ptr[dev] = p;
+  }
+  *out = reinterpret_cast<L1Chan*>(g_l1ball_scratch_ptr[dev]);
+  return DTV_OK;
+}
+
+}  // namespace dtv
+
+extern "C" int dtv_l1ball_noalloc(const float* v, float* w, int64_t n, const double* radius,
+                                  double* lambda_out, void* stream) {
+  using namespace dtv;
+  DTV_CHECK(v && w && radius, "NULL argument");
+  DTV_CHECK(n > 0, "n must be positive");
+  DTV_CHECK(n <= kL1NoallocMaxN,
+            "n = %lld exceeds the maximum %lld elements of dtv_l1ball_noalloc",
+            (long long)n, (long long)kL1NoallocMaxN);
+  L1Chan* ch = nullptr;
+  int rc = l1ball_scratch(&ch);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  // The array keeps whatever the previous call left; the histograms must
+  // start at zero, so clear the whole workspace first.
+  DTV_CUDA_TRY(cudaMemsetAsync(ch, 0, sizeof(L1Chan), st));
+  l1_reset_kernel<<<1, 32, 0, st>>>(ch, 1, radius, nullptr, 0.f, 0.f, 0.f); note_launch();
+  l1_hist1_kernel<<<blocks_for(n, 256, 4), 256, 0, st>>>(v, n, ch); note_launch();
+  l1_select_kernel<<<1, 1024, 0, st>>>(ch, 1); note_launch();
+  l1_hist_kernel<1><<<blocks_for(n, 256, 4), 256, 0, st>>>(v, nullptr, nullptr, n, ch, 2); note_launch();
+  l1_select_kernel<<<1, 1024, 0, st>>>(ch, 2); note_launch();
+  l1_hist_kernel<1><<<blocks_for(n, 256, 4), 256, 0, st>>>(v, nullptr, nullptr, n, ch, 3); note_launch();
+  l1_select_kernel<<<1, 1024, 0, st>>>(ch, 3); note_launch();
+  l1_apply_kernel<<<blocks_for(n), 256, 0, st>>>(v, w, n, ch, lambda_out); note_launch();
+  DTV_LAUNCH_CHECK();
+  return DTV_OK;
+}

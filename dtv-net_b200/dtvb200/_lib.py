@@ -80,6 +80,7 @@ SIGNATURES = {
     "dtv_diff_abs_sums": [_P, _I, _IP, _I, _I, _P, _P],
     "dtv_l1ball_workspace_bytes": [],
     "dtv_l1ball": [_P, _P, _L, _P, _P, _P, _P],
+    "dtv_l1ball_noalloc": [_P, _P, _L, _P, _P, _P],
     "dtv_pdhg_workspace_bytes": [],
     "dtv_pdhg_dual": [_P, _P, _P, _P, _P, _IP, _I, ctypes.POINTER(dtv_pdhg_params), _P, _P, _P],
     "dtv_pdhg_primal": [_P, _P, _P, _P, _P, _P, _P, _IP, _I, ctypes.POINTER(dtv_pdhg_params),

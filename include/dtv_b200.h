@@ -223,6 +223,21 @@ DTV_API int64_t dtv_l1ball_workspace_bytes(void);
 DTV_API int dtv_l1ball(const float* v, float* w, int64_t n, const double* radius, void* workspace,
                double* lambda_out, void* stream);
 
+/* dtv_l1ball for callers that cannot allocate device memory where they
+ * project (a host that reserves the GPU up front and exposes no allocator, a
+ * C/Fortran caller without a device allocator, a loop that must not call
+ * cudaMalloc/cudaFree because cudaFree synchronises the device). No
+ * counterpart in the reference. Same arguments and result as dtv_l1ball minus
+ * the workspace: the search runs in a 49,200-byte array compiled into the
+ * library (one per GPU, held until the process exits). n must not exceed
+ * 2^31-1 (larger n returns DTV_ERR_INVALID). The first call on each device
+ * looks up that array's address; make the first call before any stream
+ * capture. All calls on a device share the array, so calls that overlap on
+ * the GPU (different streams, or different host threads) race; each call
+ * clears it before use. Allocates nothing. */
+DTV_API int dtv_l1ball_noalloc(const float* v, float* w, int64_t n, const double* radius,
+                               double* lambda_out, void* stream);
+
 /* ---- DTV by Chambolle-Pock (model/PDHG/DTVCP.py:29-60) ------------------------- */
 typedef struct dtv_pdhg_params {
   float sigma;  /* dual step (DTVCP.py:27)                    */
