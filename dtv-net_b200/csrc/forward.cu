@@ -48,7 +48,10 @@ struct RaySetup {
   int count;
 };
 
-__device__ __forceinline__ RaySetup setup_ray(const RayParams& rp, const FPView& f, int u, int v) {
+// `shift` is added to the start position (1/2 for texture coordinates, whose
+// texel centres sit at i + 1/2).
+__device__ __forceinline__ RaySetup setup_ray(const RayParams& rp, const FPView& f, int u, int v,
+                                              float shift = 0.f) {
   RaySetup rs;
   double r[3], rw[3];
 #pragma unroll
@@ -125,7 +128,7 @@ __device__ __forceinline__ RaySetup setup_ray(const RayParams& rp, const FPView&
   const double ab = a0 + kb * rp.step;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    rs.p0[c] = (float)(f.s[c] + ab * d[c]);
+    rs.p0[c] = (float)(f.s[c] + ab * d[c] + shift);
     rs.dp[c] = (float)(d[c] * rp.step);
   }
   return rs;
@@ -155,10 +158,11 @@ struct SoftSampler {
   }
 };
 
+// Texture coordinates: the ray set-up already added the 1/2 texel offset.
 struct TexSampler {
   cudaTextureObject_t tex;
   __device__ __forceinline__ float operator()(float x, float y, float z) const {
-    return tex3D<float>(tex, x + 0.5f, y + 0.5f, z + 0.5f);
+    return tex3D<float>(tex, x, y, z);
   }
 };
 
@@ -195,23 +199,27 @@ __device__ __forceinline__ void block_add_double(double val, double* dst) {
 
 template <class Sampler>
 __device__ __forceinline__ float ray_sum(const Sampler& smp, const RaySetup& rs) {
-  float acc = 0.f;
+  float a0 = 0.f, a1 = 0.f;
   int k = 0;
-  for (; k + 1 < rs.count; k += 2) {
-    const float k0 = (float)k, k1 = (float)(k + 1);
-    const float s0 = smp(fmaf(k0, rs.dp[0], rs.p0[0]), fmaf(k0, rs.dp[1], rs.p0[1]),
-                         fmaf(k0, rs.dp[2], rs.p0[2]));
-    const float s1 = smp(fmaf(k1, rs.dp[0], rs.p0[0]), fmaf(k1, rs.dp[1], rs.p0[1]),
-                         fmaf(k1, rs.dp[2], rs.p0[2]));
-    acc += s0;
-    acc += s1;
+  for (; k + 3 < rs.count; k += 4) {
+    float s[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float kf = (float)(k + j);
+      s[j] = smp(fmaf(kf, rs.dp[0], rs.p0[0]), fmaf(kf, rs.dp[1], rs.p0[1]),
+                 fmaf(kf, rs.dp[2], rs.p0[2]));
+    }
+    a0 += s[0];
+    a1 += s[1];
+    a0 += s[2];
+    a1 += s[3];
   }
-  if (k < rs.count) {
+  for (; k < rs.count; ++k) {
     const float kf = (float)k;
-    acc += smp(fmaf(kf, rs.dp[0], rs.p0[0]), fmaf(kf, rs.dp[1], rs.p0[1]),
-               fmaf(kf, rs.dp[2], rs.p0[2]));
+    a0 += smp(fmaf(kf, rs.dp[0], rs.p0[0]), fmaf(kf, rs.dp[1], rs.p0[1]),
+              fmaf(kf, rs.dp[2], rs.p0[2]));
   }
-  return acc;
+  return a0 + a1;
 }
 
 template <class T>
@@ -253,7 +261,7 @@ __global__ void __launch_bounds__(kFPThreads) fp_tex_kernel(RayParams rp, const 
   const int n = blockIdx.y, b = blockIdx.z;
   float res = 0.f;
   if (u < rp.nu && v < rp.nv) {
-    const RaySetup rs = setup_ray(rp, views[n], u, v);
+    const RaySetup rs = setup_ray(rp, views[n], u, v, 0.5f);
     TexSampler smp{texs[b]};
     const float val = rs.count > 0 ? ray_sum(smp, rs) * rp.scale : 0.f;
     const int64_t idx = ((int64_t)b * rp.n_views + n) * rp.nu * rp.nv + (int64_t)v * rp.nu + u;

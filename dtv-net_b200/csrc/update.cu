@@ -5,13 +5,15 @@
 // operator is a sparse matrix D = shift - I: row i is -e_i plus e_{i+o} when
 // row i is "valid" (x: (i+1) % X != 0; y: i < N - size[1], with offset
 // size[1]; z: i < N - X*Y). The stencils below apply those matrices and their
-// transposes without building them.
+// transposes without building them. Volume kernels run on a (x, y, z-slab)
+// grid: a warp is 32 consecutive x of one row, and each thread marches
+// kZS slices along z, carrying the z-neighbour from one slice to the next.
 //
 // The L1-ball projection (model/PDHG/Utils/L1ball.py:4-17) needs the threshold
 // lambda solving sum_i max(a_i - lambda, 0) = r. The reference Newton-iterates
 // lambda with a host sync per step. Here it is found exactly by a three-level
 // radix search over the IEEE-754 bit patterns of a_i >= 0 (monotone in a_i):
-// 2048 / 1024 / 1024 bins on key bits [30:20] / [19:10] / [9:0]. Every bin of
+// 1024 / 1024 / 2048 bins on key bits [30:21] / [20:11] / [10:0]. Every bin of
 // a level shares one exponent, so its sum is kept exactly as an integer sum of
 // 24-bit significands. After the last level the bin is a single value and
 // lambda follows in closed form from the counts and sums above it.
@@ -44,6 +46,46 @@ static Dims make_dims(const int32_t s[3], int quirk) {
   return d;
 }
 
+constexpr int kTX = 32, kTY = 8, kZS = 8;  // block 32 x 8 threads, 8 slices per thread
+
+static int check_dims(const int32_t s[3], int batch) {
+  DTV_CHECK(s != nullptr, "NULL size");
+  DTV_CHECK(s[0] > 0 && s[1] > 0 && s[2] > 0 && batch > 0, "bad size (%d,%d,%d) x %d", s[0],
+            s[1], s[2], batch);
+  DTV_CHECK((int64_t)((s[2] + kZS - 1) / kZS) * batch <= 65535,
+            "z slabs x batch exceeds the grid limit");
+  DTV_CHECK((s[1] + kTY - 1) / kTY <= 65535, "ny too large");
+  DTV_CHECK((int64_t)s[0] * s[1] * s[2] <= 2147483647LL, "volume exceeds 2^31-1 voxels");
+  return DTV_OK;
+}
+
+static dim3 grid3(const Dims& d, int batch) {
+  return dim3((d.X + kTX - 1) / kTX, (d.Y + kTY - 1) / kTY, ((d.Z + kZS - 1) / kZS) * batch);
+}
+static const dim3 kBlock3(kTX, kTY);
+
+// Position of this thread: column (x, y) of batch item b, slices [z0, z0+kZS).
+struct Col {
+  int x, y, z0, nz;  // nz = slices this thread handles
+  int64_t base;      // b * N
+  bool in;
+};
+__device__ __forceinline__ Col col3(const Dims& d) {
+  Col c;
+  c.x = blockIdx.x * kTX + threadIdx.x;
+  c.y = blockIdx.y * kTY + threadIdx.y;
+  const int zslabs = (d.Z + kZS - 1) / kZS;
+  const int zb = blockIdx.z % zslabs;
+  const int b = blockIdx.z / zslabs;
+  c.z0 = zb * kZS;
+  c.nz = min(kZS, d.Z - c.z0);
+  c.base = (int64_t)b * d.N;
+  c.in = c.x < d.X && c.y < d.Y;
+  return c;
+}
+__device__ __forceinline__ int ltid() { return threadIdx.y * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ int lthreads() { return blockDim.x * blockDim.y; }
+
 __device__ __forceinline__ int64_t axis_off(const Dims& d, int a) {
   return a == 0 ? 1 : (a == 1 ? (d.quirk ? d.Y : d.X) : (int64_t)d.X * d.Y);
 }
@@ -67,11 +109,17 @@ __device__ __forceinline__ float dfwd(const T* f, const Dims& d, int a, int64_t 
   return row_valid(d, a, i, x, y, z) ? load_as_float(f, i + axis_off(d, a)) - c : -c;
 }
 
+// (x, y, z) of flat index i inside one item (i < 2^31, checked on the host);
+// used only for the few neighbour rows that need it
 __device__ __forceinline__ void decompose(const Dims& d, int64_t i, int& x, int& y, int& z) {
-  x = (int)(i % d.X);
-  const int64_t r = i / d.X;
-  y = (int)(r % d.Y);
-  z = (int)(r / d.Y);
+  const unsigned int ii = (unsigned int)i;
+  const unsigned int plane = (unsigned int)d.X * (unsigned int)d.Y;
+  const unsigned int zz = ii / plane;
+  const unsigned int r = ii - zz * plane;
+  const unsigned int yy = r / (unsigned int)d.X;
+  z = (int)zz;
+  y = (int)yy;
+  x = (int)(r - yy * (unsigned int)d.X);
 }
 
 // ---- warp / block reductions ------------------------------------------------------------
@@ -84,14 +132,14 @@ __device__ __forceinline__ double warp_sum(double v) {
 template <int C>
 __device__ __forceinline__ void block_sums_atomic(double (&v)[C], double* dst) {
   __shared__ double red[C][32];
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int t = ltid(), w = t >> 5, l = t & 31, nw = lthreads() >> 5;
 #pragma unroll
   for (int c = 0; c < C; ++c) {
     v[c] = warp_sum(v[c]);
     if (l == 0) red[c][w] = v[c];
   }
   __syncthreads();
-  if (threadIdx.x < 32) {
+  if (t < 32) {
 #pragma unroll
     for (int c = 0; c < C; ++c) {
       double s = l < nw ? red[c][l] : 0.0;
@@ -102,43 +150,48 @@ __device__ __forceinline__ void block_sums_atomic(double (&v)[C], double* dst) {
 }
 
 // ---- finite differences ---------------------------------------------------------------------
-__global__ void diff_kernel(const float* __restrict__ f, float* __restrict__ out, Dims d,
-                            int64_t total, int a, int transpose) {
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t b = t / d.N, i = t - b * d.N;
-    int x, y, z;
-    decompose(d, i, x, y, z);
-    const float* fb = f + b * d.N;
+__global__ void __launch_bounds__(256) diff_kernel(const float* __restrict__ f, float* __restrict__ out,
+                                                   Dims d, int a, int transpose) {
+  const Col c = col3(d);
+  if (!c.in) return;
+  const float* fb = f + c.base;
+  for (int k = 0; k < c.nz; ++k) {
+    const int z = c.z0 + k;
+    const int64_t i = ((int64_t)z * d.Y + c.y) * d.X + c.x;
     float r;
     if (!transpose) {
-      r = dfwd(fb, d, a, i, x, y, z);
+      r = dfwd(fb, d, a, i, c.x, c.y, z);
     } else {
       r = -__ldg(fb + i);
-      if (col_valid(d, a, i, x, y, z)) r += __ldg(fb + i - axis_off(d, a));
+      if (col_valid(d, a, i, c.x, c.y, z)) r += __ldg(fb + i - axis_off(d, a));
     }
-    out[t] = r;
+    out[c.base + i] = r;
   }
 }
 
 template <class T>
-__global__ void diff_abs_sums_kernel(const T* __restrict__ f, Dims d, int64_t total,
-                                     double* __restrict__ sums) {
+__global__ void __launch_bounds__(256) diff_abs_sums_kernel(const T* __restrict__ f, Dims d,
+                                                            double* __restrict__ sums) {
+  const Col c = col3(d);
   double acc[3] = {0.0, 0.0, 0.0};
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t b = t / d.N, i = t - b * d.N;
-    int x, y, z;
-    decompose(d, i, x, y, z);
-    const T* fb = f + b * d.N;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) acc[a] += fabsf(dfwd(fb, d, a, i, x, y, z));
+  if (c.in) {
+    const T* fb = f + c.base;
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+    for (int k = 0; k < c.nz; ++k) {
+      const int z = c.z0 + k;
+      const int64_t i = ((int64_t)z * d.Y + c.y) * d.X + c.x;
+      s0 += fabsf(dfwd(fb, d, 0, i, c.x, c.y, z));
+      s1 += fabsf(dfwd(fb, d, 1, i, c.x, c.y, z));
+      s2 += fabsf(dfwd(fb, d, 2, i, c.x, c.y, z));
+    }
+    acc[0] = s0; acc[1] = s1; acc[2] = s2;
   }
   block_sums_atomic<3>(acc, sums);
 }
 
 // ---- L1-ball radix search ------------------------------------------------------------------
-constexpr int kL1Bins1 = 2048, kL1Bins2 = 1024, kL1Bins3 = 1024;
+constexpr int kL1B1 = 1024, kL1B2 = 1024, kL1B3 = 2048;
+constexpr int kL1S1 = 21, kL1S2 = 11;  // key >> 21: level-1 bin; >> 11: level-2 prefix
 
 struct L1Chan {
   double radius;
@@ -149,14 +202,15 @@ struct L1Chan {
   unsigned int maxkey;
   int done;
   float thresh;
-  unsigned int cnt1[kL1Bins1];
-  unsigned int cnt2[kL1Bins2];
-  unsigned int cnt3[kL1Bins3];
-  unsigned long long sum1[kL1Bins1];
-  unsigned long long sum2[kL1Bins2];
-  unsigned long long sum3[kL1Bins3];
+  unsigned int cnt1[kL1B1];
+  unsigned int cnt2[kL1B2];
+  unsigned int cnt3[kL1B3];
+  unsigned long long sum1[kL1B1];
+  unsigned long long sum2[kL1B2];
+  unsigned long long sum3[kL1B3];
 };
 static_assert(sizeof(L1Chan) % 16 == 0, "L1Chan alignment");
+static_assert(sizeof(L1Chan) == 49200, "L1Chan size is part of the documented interface");
 
 __device__ __forceinline__ unsigned int sig24(unsigned int key) {
   const unsigned int m = key & 0x7FFFFFu;
@@ -171,16 +225,15 @@ __device__ __forceinline__ void hist_add(unsigned int* cnt, unsigned long long* 
   if (!active) return;
   const unsigned int grp = __match_any_sync(act, bin);
   const unsigned int s = __reduce_add_sync(grp, sig24(key));
-  if ((threadIdx.x & 31) == (unsigned)(__ffs(grp) - 1)) {
+  if ((ltid() & 31) == __ffs(grp) - 1) {
     atomicAdd(cnt + bin, (unsigned int)__popc(grp));
     atomicAdd(sum + bin, (unsigned long long)s);
   }
 }
 
-template <int NB>
 __device__ __forceinline__ void hist_flush(const unsigned int* scnt, const unsigned long long* ssum,
-                                           unsigned int* gcnt, unsigned long long* gsum) {
-  for (int i = threadIdx.x; i < NB; i += blockDim.x) {
+                                           unsigned int* gcnt, unsigned long long* gsum, int nb) {
+  for (int i = ltid(); i < nb; i += lthreads()) {
     if (scnt[i]) {
       atomicAdd(gcnt + i, scnt[i]);
       atomicAdd(gsum + i, ssum[i]);
@@ -188,61 +241,96 @@ __device__ __forceinline__ void hist_flush(const unsigned int* scnt, const unsig
   }
 }
 
-// Level-2 / level-3 histogram pass over C channels (keys of |x|).
+// Level-2 / level-3 histogram pass over one channel (keys of |x|), static
+// shared memory for the largest (level-3) bin count.
 template <int C>
 __global__ void l1_hist_kernel(const float* __restrict__ x0, const float* __restrict__ x1,
                                const float* __restrict__ x2, int64_t n, L1Chan* chans, int level) {
-  __shared__ unsigned int scnt[C][1024];
-  __shared__ unsigned long long ssum[C][1024];
-  bool any = false;
-#pragma unroll
-  for (int c = 0; c < C; ++c) any |= !chans[c].done;
-  if (!any) return;
-  for (int i = threadIdx.x; i < 1024; i += blockDim.x)
-#pragma unroll
-    for (int c = 0; c < C; ++c) {
-      scnt[c][i] = 0;
-      ssum[c][i] = 0;
-    }
-  unsigned int pre[C];
-  bool live[C];
-#pragma unroll
-  for (int c = 0; c < C; ++c) {
-    pre[c] = chans[c].prefix;
-    live[c] = !chans[c].done;
+  static_assert(C == 1, "one channel");
+  __shared__ unsigned int scnt[kL1B3];
+  __shared__ unsigned long long ssum[kL1B3];
+  L1Chan& ch = chans[0];
+  if (ch.done) return;
+  const int nb = level == 2 ? kL1B2 : kL1B3;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+    scnt[i] = 0;
+    ssum[i] = 0;
   }
+  const unsigned int pre = ch.prefix;
+  const int pshift = level == 2 ? kL1S1 : kL1S2;
   __syncthreads();
-  const int pshift = level == 2 ? 20 : 10;
-  const float* xs[3] = {x0, x1, x2};
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t nround = (n + stride - 1) / stride * stride;  // all lanes iterate together
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nround; t += stride) {
+    unsigned int key = 0;
+    bool act = false;
+    if (t < n) {
+      key = __float_as_uint(__ldg(x0 + t)) & 0x7FFFFFFFu;
+      act = (key >> pshift) == pre;
+    }
+    const int bin = level == 2 ? (int)((key >> kL1S2) & (kL1B2 - 1)) : (int)(key & (kL1B3 - 1));
+    hist_add(scnt, ssum, bin, key, act);
+  }
+  __syncthreads();
+  if (level == 2) hist_flush(scnt, ssum, ch.cnt2, ch.sum2, kL1B2);
+  else hist_flush(scnt, ssum, ch.cnt3, ch.sum3, kL1B3);
+}
+
+// Level-2 or level-3 pass over three channels at once (the fused PDHG path);
+// dynamic shared memory: 3 x bins x 12 bytes.
+__global__ void __launch_bounds__(512) l1_hist3_kernel(const float* __restrict__ x0,
+                                                       const float* __restrict__ x1,
+                                                       const float* __restrict__ x2, int64_t n,
+                                                       L1Chan* chans, int level) {
+  extern __shared__ unsigned char smem[];
+  const int nb = level == 2 ? kL1B2 : kL1B3;
+  unsigned int* scnt = reinterpret_cast<unsigned int*>(smem);
+  unsigned long long* ssum = reinterpret_cast<unsigned long long*>(smem + 3 * nb * 4);
+  bool live[3];
+  unsigned int pre[3];
 #pragma unroll
-    for (int c = 0; c < C; ++c) {
+  for (int c = 0; c < 3; ++c) {
+    live[c] = !chans[c].done;
+    pre[c] = chans[c].prefix;
+  }
+  if (!live[0] && !live[1] && !live[2]) return;
+  for (int i = threadIdx.x; i < 3 * nb; i += blockDim.x) {
+    scnt[i] = 0;
+    ssum[i] = 0;
+  }
+  __syncthreads();
+  const int pshift = level == 2 ? kL1S1 : kL1S2;
+  const float* xs[3] = {x0, x1, x2};
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t nround = (n + stride - 1) / stride * stride;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nround; t += stride) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
       unsigned int key = 0;
       bool act = false;
       if (t < n && live[c]) {
         key = __float_as_uint(__ldg(xs[c] + t)) & 0x7FFFFFFFu;
         act = (key >> pshift) == pre[c];
       }
-      const int bin = level == 2 ? (int)((key >> 10) & 1023u) : (int)(key & 1023u);
-      hist_add(scnt[c], ssum[c], bin, key, act);
+      const int bin =
+          level == 2 ? (int)((key >> kL1S2) & (kL1B2 - 1)) : (int)(key & (kL1B3 - 1));
+      hist_add(scnt + c * nb, ssum + c * nb, bin, key, act);
     }
   }
   __syncthreads();
 #pragma unroll
-  for (int c = 0; c < C; ++c) {
+  for (int c = 0; c < 3; ++c) {
     if (!live[c]) continue;
-    if (level == 2) hist_flush<1024>(scnt[c], ssum[c], chans[c].cnt2, chans[c].sum2);
-    else hist_flush<1024>(scnt[c], ssum[c], chans[c].cnt3, chans[c].sum3);
+    if (level == 2) hist_flush(scnt + c * nb, ssum + c * nb, chans[c].cnt2, chans[c].sum2, nb);
+    else hist_flush(scnt + c * nb, ssum + c * nb, chans[c].cnt3, chans[c].sum3, nb);
   }
 }
 
 // Level-1 histogram of a plain array (standalone L1-ball).
 __global__ void l1_hist1_kernel(const float* __restrict__ v, int64_t n, L1Chan* ch) {
-  __shared__ unsigned int scnt[kL1Bins1];
-  __shared__ unsigned long long ssum[kL1Bins1];
-  for (int i = threadIdx.x; i < kL1Bins1; i += blockDim.x) {
+  __shared__ unsigned int scnt[kL1B1];
+  __shared__ unsigned long long ssum[kL1B1];
+  for (int i = threadIdx.x; i < kL1B1; i += blockDim.x) {
     scnt[i] = 0;
     ssum[i] = 0;
   }
@@ -254,10 +342,10 @@ __global__ void l1_hist1_kernel(const float* __restrict__ v, int64_t n, L1Chan* 
     unsigned int key = 0;
     if (t < n) key = __float_as_uint(__ldg(v + t)) & 0x7FFFFFFFu;
     kmax = max(kmax, key);
-    hist_add(scnt, ssum, (int)(key >> 20), key, t < n);
+    hist_add(scnt, ssum, (int)(key >> kL1S1), key, t < n);
   }
   __syncthreads();
-  hist_flush<kL1Bins1>(scnt, ssum, ch->cnt1, ch->sum1);
+  hist_flush(scnt, ssum, ch->cnt1, ch->sum1, kL1B1);
   for (int o = 16; o > 0; o >>= 1) kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
   if ((threadIdx.x & 31) == 0 && kmax) atomicMax(&ch->maxkey, kmax);
 }
@@ -273,14 +361,15 @@ __device__ __forceinline__ double bin_scale(unsigned int key_lo) {
 __global__ void __launch_bounds__(1024) l1_select_kernel(L1Chan* chans, int level) {
   L1Chan& ch = chans[blockIdx.x];
   if (ch.done) return;
-  const int nb = level == 1 ? kL1Bins1 : (level == 2 ? kL1Bins2 : kL1Bins3);
+  const int nb = level == 1 ? kL1B1 : (level == 2 ? kL1B2 : kL1B3);
   unsigned int* cnt = level == 1 ? ch.cnt1 : (level == 2 ? ch.cnt2 : ch.cnt3);
   unsigned long long* sum = level == 1 ? ch.sum1 : (level == 2 ? ch.sum2 : ch.sum3);
-  const int per = nb / 1024;  // 2 or 1 bins per thread, thread t owns bins [t*per, t*per+per)
-  const unsigned int kbase = level == 1 ? 0u : (level == 2 ? (ch.prefix << 20) : (ch.prefix << 10));
-  const int bshift = level == 1 ? 20 : (level == 2 ? 10 : 0);
+  const int per = nb / 1024;  // 1 or 2 bins per thread, thread t owns bins [t*per, t*per+per)
+  const unsigned int kbase =
+      level == 1 ? 0u : (level == 2 ? (ch.prefix << kL1S1) : (ch.prefix << kL1S2));
+  const int bshift = level == 1 ? kL1S1 : (level == 2 ? kL1S2 : 0);
   double c_loc = 0.0, t_loc = 0.0;
-  double cb[2], tb[2];
+  double cb[2] = {0.0, 0.0}, tb[2] = {0.0, 0.0};
   const int t = threadIdx.x;
   for (int q = 0; q < per; ++q) {
     const int j = t * per + q;
@@ -316,17 +405,12 @@ __global__ void __launch_bounds__(1024) l1_select_kernel(L1Chan* chans, int leve
     t_hi += wt[ww];
   }
   // C/T over bins strictly above this thread's bins, plus what earlier levels fixed
-  double c_above = ch.c_above + c_hi + (c_s - c_loc);
-  double t_above = ch.t_above + t_hi + (t_s - t_loc);
+  const double c_above = ch.c_above + c_hi + (c_s - c_loc);
+  const double t_above = ch.t_above + t_hi + (t_s - t_loc);
   const double radius = ch.radius;
   if (level == 1 && t == 0) {
-    // totals for the special cases
-    double ctot = 0.0, ttot = 0.0;
-    for (int ww = 0; ww < 32; ++ww) {
-      ctot += wc[ww];
-      ttot += wt[ww];
-    }
-    (void)ctot;
+    double ttot = 0.0;
+    for (int ww = 0; ww < 32; ++ww) ttot += wt[ww];
     if (ttot < radius) {  // sum|v| < b: the reference returns v (L1ball.py:5-6)
       ch.done = 1;
       ch.thresh = 0.f;
@@ -387,8 +471,8 @@ __global__ void __launch_bounds__(1024) l1_select_kernel(L1Chan* chans, int leve
   }
 }
 
-// Resets a channel for a new search (radius from a device double, optionally
-// scaled and multiplied by a device constraint level).
+// Resets channels for a new search: radius from device doubles, or
+// s_c * t[c] (a scale times a device constraint level).
 __global__ void l1_reset_kernel(L1Chan* chans, int C, const double* radius, const double* t,
                                 float s0, float s1, float s2) {
   const int c = threadIdx.x;
@@ -421,85 +505,95 @@ __global__ void l1_apply_kernel(const float* __restrict__ v, float* __restrict__
 template <class T>
 __global__ void __launch_bounds__(256) pdhg_dual_kernel(const T* __restrict__ fbar, float* __restrict__ p,
                                                         float* __restrict__ q, float* __restrict__ s,
-                                                        float* __restrict__ c, Dims d, int64_t total,
-                                                        float a0, float a1, float a2, float smu,
+                                                        float* __restrict__ c, Dims d, float a0,
+                                                        float a1, float a2, float smu,
                                                         L1Chan* chans) {
-  extern __shared__ unsigned char smem[];
-  unsigned int* scnt = reinterpret_cast<unsigned int*>(smem);                      // [3][2048]
-  unsigned long long* ssum = reinterpret_cast<unsigned long long*>(smem + 3 * kL1Bins1 * 4);
-  for (int i = threadIdx.x; i < 3 * kL1Bins1; i += blockDim.x) {
-    scnt[i] = 0;
-    ssum[i] = 0;
+  __shared__ unsigned int scnt[3][kL1B1];
+  __shared__ unsigned long long ssum[3][kL1B1];
+  for (int i = ltid(); i < 3 * kL1B1; i += lthreads()) {
+    (&scnt[0][0])[i] = 0;
+    (&ssum[0][0])[i] = 0;
   }
   __syncthreads();
+  const Col cl = col3(d);
   unsigned int kmax[3] = {0u, 0u, 0u};
-  float* outs[3] = {p, q, s};
-  const float as[3] = {a0, a1, a2};
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  const int64_t nround = (total + stride - 1) / stride * stride;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nround; t += stride) {
-    const bool in = t < total;
+  const T* fb = fbar + cl.base;
+  const int64_t plane = (int64_t)d.X * d.Y;
+  const int64_t oy = axis_off(d, 1);
+  int64_t i = ((int64_t)cl.z0 * d.Y + cl.y) * d.X + cl.x;
+  float fc = cl.in ? load_as_float(fb, i) : 0.f;  // f(i), carried along z
+  for (int k = 0; k < kZS; ++k, i += plane) {
+    const bool in = cl.in && k < cl.nz;
     unsigned int key[3] = {0u, 0u, 0u};
     if (in) {
-      const int64_t b = t / d.N, i = t - b * d.N;
-      int x, y, z;
-      decompose(d, i, x, y, z);
-      const T* fb = fbar + b * d.N;
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const float g = dfwd(fb, d, a, i, x, y, z);
-        const float nv = fmaf(as[a], g, outs[a][t]);  // p + v*sigma*D fbar
-        outs[a][t] = nv;
-        key[a] = __float_as_uint(nv) & 0x7FFFFFFFu;
-        kmax[a] = max(kmax[a], key[a]);
-      }
-      const float cv = fmaf(smu, load_as_float(fb, i), c[t]);
-      c[t] = fminf(cv, 0.f);  // -relu(-c - sigma*mu*fbar)
+      const int z = cl.z0 + k;
+      const float fz = z < d.Z - 1 ? load_as_float(fb, i + plane) : 0.f;
+      const float gx = cl.x < d.X - 1 ? load_as_float(fb, i + 1) - fc : -fc;
+      const bool yv = d.quirk ? (i < d.N - d.Y) : (cl.y < d.Y - 1);
+      const float gy = yv ? load_as_float(fb, i + oy) - fc : -fc;
+      const float gz = z < d.Z - 1 ? fz - fc : -fc;
+      const int64_t t = cl.base + i;
+      const float np = fmaf(a0, gx, p[t]), nq = fmaf(a1, gy, q[t]), ns = fmaf(a2, gz, s[t]);
+      p[t] = np;
+      q[t] = nq;
+      s[t] = ns;
+      c[t] = fminf(fmaf(smu, fc, c[t]), 0.f);  // -relu(-c - sigma*mu*fbar)
+      key[0] = __float_as_uint(np) & 0x7FFFFFFFu;
+      key[1] = __float_as_uint(nq) & 0x7FFFFFFFu;
+      key[2] = __float_as_uint(ns) & 0x7FFFFFFFu;
+      kmax[0] = max(kmax[0], key[0]);
+      kmax[1] = max(kmax[1], key[1]);
+      kmax[2] = max(kmax[2], key[2]);
+      fc = fz;
     }
 #pragma unroll
-    for (int a = 0; a < 3; ++a)
-      hist_add(scnt + a * kL1Bins1, ssum + a * kL1Bins1, (int)(key[a] >> 20), key[a], in);
+    for (int a = 0; a < 3; ++a) hist_add(scnt[a], ssum[a], (int)(key[a] >> kL1S1), key[a], in);
   }
   __syncthreads();
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    hist_flush<kL1Bins1>(scnt + a * kL1Bins1, ssum + a * kL1Bins1, chans[a].cnt1, chans[a].sum1);
+    hist_flush(scnt[a], ssum[a], chans[a].cnt1, chans[a].sum1, kL1B1);
     unsigned int km = kmax[a];
     for (int o = 16; o > 0; o >>= 1) km = max(km, __shfl_xor_sync(0xffffffffu, km, o));
-    if ((threadIdx.x & 31) == 0 && km) atomicMax(&chans[a].maxkey, km);
+    if ((ltid() & 31) == 0 && km) atomicMax(&chans[a].maxkey, km);
   }
 }
 
 __device__ __forceinline__ float clipf(float x, float m) { return copysignf(fminf(fabsf(x), m), x); }
 
 // ---- fused PDHG primal step (DTVCP.py:44-54) ----------------------------------------------------
+// The duals are clipped in place; neighbours may read a value before or after
+// its clip, and clipping is idempotent, so both give the same result.
 template <class T>
 __global__ void __launch_bounds__(256) pdhg_primal_kernel(T* __restrict__ f, T* __restrict__ fbar,
                                                           const float* __restrict__ recon, float* p,
                                                           float* q, float* s,
                                                           const float* __restrict__ c, Dims d,
-                                                          int64_t total, float tau, float mu,
-                                                          float v0, float v1, float v2,
-                                                          const L1Chan* chans) {
+                                                          float tau, float mu, float v0, float v1,
+                                                          float v2, const L1Chan* chans) {
+  const Col cl = col3(d);
+  if (!cl.in) return;
   const float m0 = chans[0].thresh, m1 = chans[1].thresh, m2 = chans[2].thresh;
-  float* duals[3] = {p, q, s};
-  const float ms[3] = {m0, m1, m2};
-  const float vs[3] = {v0, v1, v2};
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t b = t / d.N, i = t - b * d.N;
-    int x, y, z;
-    decompose(d, i, x, y, z);
-    float reg = mu * c[t];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      float* g = duals[a] + b * d.N;
-      const float self = clipf(g[i], ms[a]);
-      float dt = -self;
-      if (col_valid(d, a, i, x, y, z)) dt += clipf(g[i - axis_off(d, a)], ms[a]);
-      reg = fmaf(vs[a], dt, reg);
-      g[i] = self;  // idempotent: neighbours re-clip whatever they read
-    }
+  const int64_t plane = (int64_t)d.X * d.Y;
+  const int64_t oy = axis_off(d, 1);
+  float* pb = p + cl.base;
+  float* qb = q + cl.base;
+  float* sb = s + cl.base;
+  int64_t i = ((int64_t)cl.z0 * d.Y + cl.y) * d.X + cl.x;
+  float sprev = cl.z0 >= 1 ? clipf(sb[i - plane], m2) : 0.f;  // s(i - XY), carried along z
+  for (int k = 0; k < cl.nz; ++k, i += plane) {
+    const float ps = clipf(pb[i], m0), qs = clipf(qb[i], m1), ss = clipf(sb[i], m2);
+    float dx = -ps, dy = -qs, dz = -ss;
+    if (cl.x >= 1) dx += clipf(pb[i - 1], m0);
+    const bool yv = d.quirk ? (i >= d.Y) : (cl.y >= 1);
+    if (yv) dy += clipf(qb[i - oy], m1);
+    if (cl.z0 + k >= 1) dz += sprev;
+    pb[i] = ps;
+    qb[i] = qs;
+    sb[i] = ss;
+    sprev = ss;
+    const int64_t t = cl.base + i;
+    const float reg = fmaf(v0, dx, fmaf(v1, dy, fmaf(v2, dz, mu * c[t])));
     const float fo = load_as_float(f, t);
     const float fn = fo - recon[t] - tau * reg;
     store_from_float(fbar, t, 2.f * fn - fo);
@@ -528,23 +622,25 @@ __global__ void relu_step_kernel(const float* __restrict__ f, const float* bp, f
     z[t] = fmaxf(f[t] - sigma * bp[t], 0.f);
 }
 
-__global__ void dtvfista_maxes_kernel(const float* __restrict__ z, Dims d, int64_t total,
-                                      unsigned int* maxbits) {
+__global__ void __launch_bounds__(256) dtvfista_maxes_kernel(const float* __restrict__ z, Dims d,
+                                                             unsigned int* maxbits) {
+  const Col c = col3(d);
   unsigned int km[3] = {0u, 0u, 0u};
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t b = t / d.N, i = t - b * d.N;
-    int x, y, zz;
-    decompose(d, i, x, y, zz);
+  if (c.in) {
+    const float* zb = z + c.base;
+    for (int k = 0; k < c.nz; ++k) {
+      const int zz = c.z0 + k;
+      const int64_t i = ((int64_t)zz * d.Y + c.y) * d.X + c.x;
 #pragma unroll
-    for (int a = 0; a < 3; ++a)
-      km[a] = max(km[a], __float_as_uint(fabsf(dfwd(z + b * d.N, d, a, i, x, y, zz))));
+      for (int a = 0; a < 3; ++a)
+        km[a] = max(km[a], __float_as_uint(fabsf(dfwd(zb, d, a, i, c.x, c.y, zz))));
+    }
   }
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     unsigned int k = km[a];
     for (int o = 16; o > 0; o >>= 1) k = max(k, __shfl_xor_sync(0xffffffffu, k, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(maxbits + a, k);
+    if ((ltid() & 31) == 0) atomicMax(maxbits + a, k);
   }
 }
 
@@ -554,17 +650,19 @@ __global__ void finish_maxes_kernel(const unsigned int* bits, float v0, float v1
   if (a < 3) maxes[a] = __uint_as_float(bits[a]) - (a == 0 ? v0 : (a == 1 ? v1 : v2));
 }
 
-__global__ void dtvfista_update_kernel(float* __restrict__ f, const float* __restrict__ z, Dims d,
-                                       int64_t total, float v0, float v1, float v2, float t0,
-                                       float t1, float t2, float mom, int quirk,
-                                       const float* __restrict__ maxes) {
+__global__ void __launch_bounds__(256) dtvfista_update_kernel(float* __restrict__ f,
+                                                              const float* __restrict__ z, Dims d,
+                                                              float v0, float v1, float v2,
+                                                              float t0, float t1, float t2,
+                                                              float mom, int quirk,
+                                                              const float* __restrict__ maxes) {
+  const Col c = col3(d);
+  if (!c.in) return;
   const float vs[3] = {v0, v1, v2}, ts[3] = {t0, t1, t2};
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t b = t / d.N, i = t - b * d.N;
-    int x, y, zz;
-    decompose(d, i, x, y, zz);
-    const float* zb = z + b * d.N;
+  const float* zb = z + c.base;
+  for (int k = 0; k < c.nz; ++k) {
+    const int zz = c.z0 + k;
+    const int64_t i = ((int64_t)zz * d.Y + c.y) * d.X + c.x;
     float fn = zb[i];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -574,8 +672,8 @@ __global__ void dtvfista_update_kernel(float* __restrict__ f, const float* __res
         const float r = fmaxf(fabsf(g) - vs[a], 0.f);
         return g > 0.f ? r : (g < 0.f ? -r : 0.f);
       };
-      float dt = -thr(dfwd(zb, d, a, i, x, y, zz));
-      if (col_valid(d, a, i, x, y, zz)) {
+      float dt = -thr(dfwd(zb, d, a, i, c.x, c.y, zz));
+      if (col_valid(d, a, i, c.x, c.y, zz)) {
         const int64_t j = i - axis_off(d, a);
         int xj, yj, zj;
         decompose(d, j, xj, yj, zj);
@@ -583,6 +681,7 @@ __global__ void dtvfista_update_kernel(float* __restrict__ f, const float* __res
       }
       fn = fmaf(ts[a], dt, fn);
     }
+    const int64_t t = c.base + i;
     const float fo = f[t];
     f[t] = fn + mom * (fn - fo);
   }
@@ -602,37 +701,40 @@ __global__ void axpy_l1_kernel(float* __restrict__ f, const float* __restrict__ 
   if (l1) block_sums_atomic<1>(acc, l1);
 }
 
-__device__ __forceinline__ void grad3(const float* f, const Dims& d, int64_t i, float g[3]) {
-  int x, y, z;
-  decompose(d, i, x, y, z);
+__device__ __forceinline__ void grad3(const float* f, const Dims& d, int64_t i, int x, int y, int z,
+                                      float g[3]) {
 #pragma unroll
   for (int a = 0; a < 3; ++a) g[a] = dfwd(f, d, a, i, x, y, z);
 }
 
-__global__ void tv_descent_kernel(const float* __restrict__ fin, float* __restrict__ fout, Dims d,
-                                  int64_t total, const float* __restrict__ davg) {
+__global__ void __launch_bounds__(256) tv_descent_kernel(const float* __restrict__ fin,
+                                                         float* __restrict__ fout, Dims d,
+                                                         const float* __restrict__ davg) {
+  const Col c = col3(d);
+  if (!c.in) return;
   const float step = davg[0];
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t b = t / d.N, i = t - b * d.N;
-    const float* fb = fin + b * d.N;
-    int x, y, z;
-    decompose(d, i, x, y, z);
+  const float* fb = fin + c.base;
+  for (int k = 0; k < c.nz; ++k) {
+    const int z = c.z0 + k;
+    const int64_t i = ((int64_t)z * d.Y + c.y) * d.X + c.x;
     float g[3];
-    grad3(fb, d, i, g);
+    grad3(fb, d, i, c.x, c.y, z, g);
     const float nrm = sqrtf(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]) + 1.f;
     float grad = 0.f;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       grad -= g[a] / nrm;
-      if (col_valid(d, a, i, x, y, z)) {
+      if (col_valid(d, a, i, c.x, c.y, z)) {
+        const int64_t j = i - axis_off(d, a);
+        int xj, yj, zj;
+        decompose(d, j, xj, yj, zj);
         float gj[3];
-        grad3(fb, d, i - axis_off(d, a), gj);
+        grad3(fb, d, j, xj, yj, zj, gj);
         const float nj = sqrtf(gj[0] * gj[0] + gj[1] * gj[1] + gj[2] * gj[2]) + 1.f;
         grad += gj[a] / nj;
       }
     }
-    fout[t] = fb[i] - step * grad;
+    fout[c.base + i] = fb[i] - step * grad;
   }
 }
 
@@ -650,11 +752,11 @@ int dtv_diff(const float* f, float* out, const int32_t size[3], int32_t batch, i
              int32_t transpose, int32_t quirk, void* stream) {
   DTV_CHECK(f && out && size, "NULL argument");
   DTV_CHECK(f != out, "dtv_diff cannot run in place");
-  DTV_CHECK(size[0] > 0 && size[1] > 0 && size[2] > 0 && batch > 0, "bad size");
+  int rc = check_dims(size, batch);
+  if (rc) return rc;
   DTV_CHECK(axis >= 0 && axis <= 2, "axis must be 0, 1 or 2");
   Dims d = make_dims(size, quirk);
-  const int64_t total = d.N * batch;
-  diff_kernel<<<blocks_for(total), 256, 0, as_stream(stream)>>>(f, out, d, total, axis, transpose); note_launch();
+  diff_kernel<<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(f, out, d, axis, transpose); note_launch();
   DTV_LAUNCH_CHECK();
   return DTV_OK;
 }
@@ -663,16 +765,15 @@ int dtv_diff_abs_sums(const void* f, int32_t dt, const int32_t size[3], int32_t 
                       int32_t quirk, double* sums, void* stream) {
   DTV_CHECK(f && sums && size, "NULL argument");
   DTV_CHECK(dt == DTV_F32 || dt == DTV_F16, "dtype must be f32 or f16");
-  DTV_CHECK(size[0] > 0 && size[1] > 0 && size[2] > 0 && batch > 0, "bad size");
+  int rc = check_dims(size, batch);
+  if (rc) return rc;
   Dims d = make_dims(size, quirk);
-  const int64_t total = d.N * batch;
   if (dt == DTV_F32) {
-    diff_abs_sums_kernel<float><<<blocks_for(total), 256, 0, as_stream(stream)>>>(
-        (const float*)f, d, total, sums); note_launch();
-  }
-  else {
-    diff_abs_sums_kernel<__half><<<blocks_for(total), 256, 0, as_stream(stream)>>>(
-        (const __half*)f, d, total, sums); note_launch();
+    diff_abs_sums_kernel<float><<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(
+        (const float*)f, d, sums); note_launch();
+  } else {
+    diff_abs_sums_kernel<__half><<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(
+        (const __half*)f, d, sums); note_launch();
   }
   DTV_LAUNCH_CHECK();
   return DTV_OK;
@@ -684,6 +785,7 @@ int dtv_l1ball(const float* v, float* w, int64_t n, const double* radius, void* 
                double* lambda_out, void* stream) {
   DTV_CHECK(v && w && radius && ws, "NULL argument");
   DTV_CHECK(n > 0, "n must be positive");
+  DTV_CHECK(n <= 2147483647LL, "n = %lld exceeds 2^31-1 (32-bit bin counts)", (long long)n);
   cudaStream_t st = as_stream(stream);
   L1Chan* ch = reinterpret_cast<L1Chan*>(ws);
   l1_reset_kernel<<<1, 32, 0, st>>>(ch, 1, radius, nullptr, 0.f, 0.f, 0.f); note_launch();
@@ -705,9 +807,11 @@ int dtv_pdhg_dual(const void* fbar, float* p, float* q, float* s, float* c, cons
                   void* stream) {
   DTV_CHECK(fbar && p && q && s && c && size && prm && t && ws, "NULL argument");
   DTV_CHECK(prm->f_dtype == DTV_F32 || prm->f_dtype == DTV_F16, "f_dtype must be f32 or f16");
-  DTV_CHECK(size[0] > 0 && size[1] > 0 && size[2] > 0 && batch > 0, "bad size");
+  int rc = check_dims(size, batch);
+  if (rc) return rc;
   Dims d = make_dims(size, prm->quirk);
   const int64_t total = d.N * batch;
+  DTV_CHECK(total <= 2147483647LL, "volume x batch exceeds 2^31-1 elements");
   cudaStream_t st = as_stream(stream);
   L1Chan* ch = reinterpret_cast<L1Chan*>(ws);
   const float sg = prm->sigma;
@@ -715,34 +819,28 @@ int dtv_pdhg_dual(const void* fbar, float* p, float* q, float* s, float* c, cons
   // onto the ball of radius v_a * t_a)
   l1_reset_kernel<<<1, 32, 0, st>>>(ch, 3, nullptr, t, sg * prm->v[0], sg * prm->v[1],
                                     sg * prm->v[2]); note_launch();
-  const size_t smem = 3 * kL1Bins1 * (sizeof(unsigned int) + sizeof(unsigned long long));
-  const int nb = blocks_for(total, 256, 2);
   if (prm->f_dtype == DTV_F32) {
-    static bool attr_f32 = false;
-    if (!attr_f32) {
-      DTV_CUDA_TRY(cudaFuncSetAttribute(pdhg_dual_kernel<float>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      attr_f32 = true;
-    }
-    pdhg_dual_kernel<float><<<nb, 256, smem, st>>>((const float*)fbar, p, q, s, c, d, total,
-                                                   prm->v[0] * sg, prm->v[1] * sg, prm->v[2] * sg,
-                                                   sg * prm->mu, ch); note_launch();
+    pdhg_dual_kernel<float><<<grid3(d, batch), kBlock3, 0, st>>>(
+        (const float*)fbar, p, q, s, c, d, prm->v[0] * sg, prm->v[1] * sg, prm->v[2] * sg,
+        sg * prm->mu, ch); note_launch();
   } else {
-    static bool attr_f16 = false;
-    if (!attr_f16) {
-      DTV_CUDA_TRY(cudaFuncSetAttribute(pdhg_dual_kernel<__half>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      attr_f16 = true;
-    }
-    pdhg_dual_kernel<__half><<<nb, 256, smem, st>>>((const __half*)fbar, p, q, s, c, d, total,
-                                                    prm->v[0] * sg, prm->v[1] * sg, prm->v[2] * sg,
-                                                    sg * prm->mu, ch); note_launch();
+    pdhg_dual_kernel<__half><<<grid3(d, batch), kBlock3, 0, st>>>(
+        (const __half*)fbar, p, q, s, c, d, prm->v[0] * sg, prm->v[1] * sg, prm->v[2] * sg,
+        sg * prm->mu, ch); note_launch();
   }
   DTV_LAUNCH_CHECK();
+  static bool attr = false;
+  const int smem3 = 3 * kL1B3 * (int)(sizeof(unsigned int) + sizeof(unsigned long long));
+  if (!attr) {
+    DTV_CUDA_TRY(cudaFuncSetAttribute(l1_hist3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      smem3));
+    attr = true;
+  }
+  const int smem2 = 3 * kL1B2 * (int)(sizeof(unsigned int) + sizeof(unsigned long long));
   l1_select_kernel<<<3, 1024, 0, st>>>(ch, 1); note_launch();
-  l1_hist_kernel<3><<<blocks_for(total, 256, 2), 256, 0, st>>>(p, q, s, total, ch, 2); note_launch();
+  l1_hist3_kernel<<<blocks_for(total, 512, 2), 512, smem2, st>>>(p, q, s, total, ch, 2); note_launch();
   l1_select_kernel<<<3, 1024, 0, st>>>(ch, 2); note_launch();
-  l1_hist_kernel<3><<<blocks_for(total, 256, 2), 256, 0, st>>>(p, q, s, total, ch, 3); note_launch();
+  l1_hist3_kernel<<<blocks_for(total, 512, 2), 512, smem3, st>>>(p, q, s, total, ch, 3); note_launch();
   l1_select_kernel<<<3, 1024, 0, st>>>(ch, 3); note_launch();
   DTV_LAUNCH_CHECK();
   return DTV_OK;
@@ -753,19 +851,18 @@ int dtv_pdhg_primal(void* f, void* fbar, const float* recon, float* p, float* q,
                     const dtv_pdhg_params* prm, const void* ws, void* stream) {
   DTV_CHECK(f && fbar && recon && p && q && s && c && size && prm && ws, "NULL argument");
   DTV_CHECK(prm->f_dtype == DTV_F32 || prm->f_dtype == DTV_F16, "f_dtype must be f32 or f16");
-  DTV_CHECK(size[0] > 0 && size[1] > 0 && size[2] > 0 && batch > 0, "bad size");
+  int rc = check_dims(size, batch);
+  if (rc) return rc;
   Dims d = make_dims(size, prm->quirk);
-  const int64_t total = d.N * batch;
   const L1Chan* ch = reinterpret_cast<const L1Chan*>(ws);
   if (prm->f_dtype == DTV_F32) {
-    pdhg_primal_kernel<float><<<blocks_for(total), 256, 0, as_stream(stream)>>>(
-        (float*)f, (float*)fbar, recon, p, q, s, c, d, total, prm->tau, prm->mu, prm->v[0],
-        prm->v[1], prm->v[2], ch); note_launch();
-  }
-  else {
-    pdhg_primal_kernel<__half><<<blocks_for(total), 256, 0, as_stream(stream)>>>(
-        (__half*)f, (__half*)fbar, recon, p, q, s, c, d, total, prm->tau, prm->mu, prm->v[0],
-        prm->v[1], prm->v[2], ch); note_launch();
+    pdhg_primal_kernel<float><<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(
+        (float*)f, (float*)fbar, recon, p, q, s, c, d, prm->tau, prm->mu, prm->v[0], prm->v[1],
+        prm->v[2], ch); note_launch();
+  } else {
+    pdhg_primal_kernel<__half><<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(
+        (__half*)f, (__half*)fbar, recon, p, q, s, c, d, prm->tau, prm->mu, prm->v[0], prm->v[1],
+        prm->v[2], ch); note_launch();
   }
   DTV_LAUNCH_CHECK();
   return DTV_OK;
@@ -789,14 +886,14 @@ int dtv_relu_step(const float* f, const float* bp, float* z, int64_t n, float si
 int dtv_dtvfista_maxes(const float* z, const int32_t size[3], int32_t batch, const float v[3],
                        float* maxes, void* stream) {
   DTV_CHECK(z && size && v && maxes, "NULL argument");
-  DTV_CHECK(size[0] > 0 && size[1] > 0 && size[2] > 0 && batch > 0, "bad size");
+  int rc = check_dims(size, batch);
+  if (rc) return rc;
   Dims d = make_dims(size, 1);
-  const int64_t total = d.N * batch;
   cudaStream_t st = as_stream(stream);
   // the three max bit patterns live in maxes[0..2] during the reduction
   unsigned int* bits = reinterpret_cast<unsigned int*>(maxes);
   DTV_CUDA_TRY(cudaMemsetAsync(bits, 0, 3 * sizeof(unsigned int), st));
-  dtvfista_maxes_kernel<<<blocks_for(total), 256, 0, st>>>(z, d, total, bits); note_launch();
+  dtvfista_maxes_kernel<<<grid3(d, batch), kBlock3, 0, st>>>(z, d, bits); note_launch();
   finish_maxes_kernel<<<1, 32, 0, st>>>(bits, v[0], v[1], v[2], maxes); note_launch();
   DTV_LAUNCH_CHECK();
   return DTV_OK;
@@ -807,11 +904,11 @@ int dtv_dtvfista_update(float* f, const float* z, const int32_t size[3], int32_t
                         const float* maxes, void* stream) {
   DTV_CHECK(f && z && size && v && t, "NULL argument");
   DTV_CHECK(!quirk || maxes, "quirk mode needs maxes");
-  DTV_CHECK(size[0] > 0 && size[1] > 0 && size[2] > 0 && batch > 0, "bad size");
+  int rc = check_dims(size, batch);
+  if (rc) return rc;
   Dims d = make_dims(size, quirk);
-  const int64_t total = d.N * batch;
-  dtvfista_update_kernel<<<blocks_for(total), 256, 0, as_stream(stream)>>>(
-      f, z, d, total, v[0], v[1], v[2], t[0], t[1], t[2], momentum, quirk, maxes); note_launch();
+  dtvfista_update_kernel<<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(
+      f, z, d, v[0], v[1], v[2], t[0], t[1], t[2], momentum, quirk, maxes); note_launch();
   DTV_LAUNCH_CHECK();
   return DTV_OK;
 }
@@ -827,10 +924,10 @@ int dtv_tv_descent(const float* f_in, float* f_out, const int32_t size[3], int32
                    int32_t quirk, const float* davg, void* stream) {
   DTV_CHECK(f_in && f_out && size && davg, "NULL argument");
   DTV_CHECK(f_in != f_out, "f_in and f_out must differ");
-  DTV_CHECK(size[0] > 0 && size[1] > 0 && size[2] > 0 && batch > 0, "bad size");
+  int rc = check_dims(size, batch);
+  if (rc) return rc;
   Dims d = make_dims(size, quirk);
-  const int64_t total = d.N * batch;
-  tv_descent_kernel<<<blocks_for(total), 256, 0, as_stream(stream)>>>(f_in, f_out, d, total, davg); note_launch();
+  tv_descent_kernel<<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(f_in, f_out, d, davg); note_launch();
   DTV_LAUNCH_CHECK();
   return DTV_OK;
 }
