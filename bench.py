@@ -195,7 +195,7 @@ def op_profile(plan, alg, img, sino, dev):
     for it in range(alg.cascades):
         if it % alg.t_refresh == 0:
             st["t"].zero_()
-            _lib.call("dtv_diff_abs_sums", _ptr(f), prm.f_dtype, size, 1, prm.quirk,
+            _lib.call("dtv_diff_abs_sums", _ptr(f), _lib.DTV_F32, size, 1, prm.quirk,
                       _ptr(st["t"]), _stream(dev))
         e = [ev() for _ in range(4)]
         e[0].record(stream)
@@ -414,7 +414,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--sampler", choices=["soft", "tex"], default="tex")
+    ap.add_argument("--sampler", choices=["soft", "tex", "pairs"], default="pairs")
     ap.add_argument("--small", action="store_true", help="64^3 smoke-size workload")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")

@@ -126,7 +126,7 @@ int backward_impl(Plan* p, const float* sino, int batch, float* out, int accumul
   bp.extent = gp.bp_extent;
   bp.scale = (float)gp.bp_scale;
   bp.sino_pad_elems = (int64_t)(gp.nu + 2 * kPad) * (gp.nv + 2 * kPad);
-  const bool tex = (p->flags & DTV_PLAN_TEX) != 0 && p->sino_tex != nullptr;
+  const bool tex = p->sino_tex != nullptr;  // allocated for the texture plans
   const int tiles = ((gp.nx + kBPTile - 1) / kBPTile) * ((gp.ny + kBPTile - 1) / kBPTile);
   dim3 grid(tiles, (gp.nz + kZC - 1) / kZC);
   const int64_t per_item = (int64_t)gp.nu * gp.nv * gp.n_views;

@@ -124,6 +124,11 @@ struct Plan {
   cudaSurfaceObject_t* vol_surf;     // staging writes into vol_arrays
   cudaArray_t* sino_arrays;
   cudaTextureObject_t* sino_tex;
+  // z-pair sampler (DTV_PLAN_TEX_PAIRS): one layered half2 array per batch item
+  cudaArray_t* pair_arrays;
+  cudaTextureObject_t* pair_tex;
+  cudaSurfaceObject_t* pair_surf;
+  cudaTextureObject_t* pair_tex_dev;
   double fp_samples;  // per volume, < 0 until computed
 };
 

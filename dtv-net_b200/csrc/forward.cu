@@ -48,10 +48,10 @@ struct RaySetup {
   int count;
 };
 
-// `shift` is added to the start position (1/2 for texture coordinates, whose
-// texel centres sit at i + 1/2).
+// `sxy` / `sz` are added to the start position's x,y / z (1/2 where the
+// sampler takes texture coordinates, whose texel centres sit at i + 1/2).
 __device__ __forceinline__ RaySetup setup_ray(const RayParams& rp, const FPView& f, int u, int v,
-                                              float shift = 0.f) {
+                                              float sxy = 0.f, float sz = 0.f) {
   RaySetup rs;
   double r[3], rw[3];
 #pragma unroll
@@ -128,7 +128,7 @@ __device__ __forceinline__ RaySetup setup_ray(const RayParams& rp, const FPView&
   const double ab = a0 + kb * rp.step;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    rs.p0[c] = (float)(f.s[c] + ab * d[c] + shift);
+    rs.p0[c] = (float)(f.s[c] + ab * d[c] + (c < 2 ? sxy : sz));
     rs.dp[c] = (float)(d[c] * rp.step);
   }
   return rs;
@@ -163,6 +163,20 @@ struct TexSampler {
   cudaTextureObject_t tex;
   __device__ __forceinline__ float operator()(float x, float y, float z) const {
     return tex3D<float>(tex, x, y, z);
+  }
+};
+
+// z-pair sampler: layer L of the half2 layered texture holds (f[L-2], f[L-1]).
+// x, y arrive as texture coordinates (shifted by 1/2), z as a voxel index.
+struct PairSampler {
+  cudaTextureObject_t tex;
+  float lmax;  // nz + 2, the last layer
+  __device__ __forceinline__ float operator()(float x, float y, float z) const {
+    const float fz = floorf(z);
+    const float w = z - fz;
+    const float L = fminf(fmaxf(fz + 2.f, 0.f), lmax);
+    const float2 a = tex2DLayered<float2>(tex, x, y, (int)L);
+    return fmaf(w, a.y - a.x, a.x);
   }
 };
 
@@ -261,7 +275,7 @@ __global__ void __launch_bounds__(kFPThreads) fp_tex_kernel(RayParams rp, const 
   const int n = blockIdx.y, b = blockIdx.z;
   float res = 0.f;
   if (u < rp.nu && v < rp.nv) {
-    const RaySetup rs = setup_ray(rp, views[n], u, v, 0.5f);
+    const RaySetup rs = setup_ray(rp, views[n], u, v, 0.5f, 0.5f);
     TexSampler smp{texs[b]};
     const float val = rs.count > 0 ? ray_sum(smp, rs) * rp.scale : 0.f;
     const int64_t idx = ((int64_t)b * rp.n_views + n) * rp.nu * rp.nv + (int64_t)v * rp.nu + u;
@@ -275,6 +289,53 @@ __global__ void __launch_bounds__(kFPThreads) fp_tex_kernel(RayParams rp, const 
     }
   }
   if (o.abs_sum) block_add_double((double)fabsf(res), o.abs_sum);
+}
+
+__global__ void __launch_bounds__(kFPThreads) fp_pair_kernel(RayParams rp, const FPView* __restrict__ views,
+                                                             const cudaTextureObject_t* texs, FPOut o) {
+  const int tiles_u = (rp.nu + kTileU - 1) / kTileU;
+  int u, v;
+  tile_pixel(tiles_u, u, v);
+  const int n = blockIdx.y, b = blockIdx.z;
+  float res = 0.f;
+  if (u < rp.nu && v < rp.nv) {
+    const RaySetup rs = setup_ray(rp, views[n], u, v, 0.5f, 0.f);
+    PairSampler smp{texs[b], (float)(rp.nz + 2)};
+    const float val = rs.count > 0 ? ray_sum(smp, rs) * rp.scale : 0.f;
+    const int64_t idx = ((int64_t)b * rp.n_views + n) * rp.nu * rp.nv + (int64_t)v * rp.nu + u;
+    if (o.epilogue == DTV_EPI_STORE) {
+      o.out[idx] = val;
+      res = val;
+    } else {
+      res = val - o.g[idx];
+      if (o.epilogue == DTV_EPI_RESIDUAL) o.out[idx] = res;
+      else o.out[idx] = (o.out[idx] + o.sigma * res) / (1.f + o.sigma);
+    }
+  }
+  if (o.abs_sum) block_add_double((double)fabsf(res), o.abs_sum);
+}
+
+// Writes the z-pair layers of one volume: layer L = (f[L-2], f[L-1]), zero
+// outside [0, nz). One thread per (x, y) column walks the nz + 3 layers.
+template <class Tin>
+__global__ void __launch_bounds__(256) stage_pairs_kernel(const Tin* __restrict__ in,
+                                                          cudaSurfaceObject_t surf, int nx, int ny,
+                                                          int nz) {
+  const int x = blockIdx.x * 32 + (threadIdx.x & 31);
+  const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
+  if (x >= nx || y >= ny) return;
+  const int64_t plane = (int64_t)nx * ny;
+  const Tin* col = in + (int64_t)y * nx + x;
+  __half prev = __float2half_rn(0.f);  // f[L-2]
+  for (int L = 0; L < nz + 3; ++L) {
+    const int z = L - 1;  // the new member f[L-1]
+    const __half cur = (z >= 0 && z < nz) ? __float2half_rn(load_as_float(col, z * plane))
+                                          : __float2half_rn(0.f);
+    const unsigned int bits = (unsigned int)__half_as_ushort(prev) |
+                              ((unsigned int)__half_as_ushort(cur) << 16);
+    surf2DLayeredwrite(bits, surf, x * 4, y, L);
+    prev = cur;
+  }
 }
 
 // ---- staging -------------------------------------------------------------------------
@@ -352,23 +413,40 @@ static int stage_volume_tex(Plan* p, const Tin* vol, int batch, cudaStream_t st)
   return DTV_OK;
 }
 
+template <class Tin>
+static int stage_volume_pairs(Plan* p, const Tin* vol, int batch, cudaStream_t st) {
+  const GeomParams& g = p->gp;
+  const int64_t vox = (int64_t)g.nx * g.ny * g.nz;
+  dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8);
+  for (int b = 0; b < batch; ++b) {
+    stage_pairs_kernel<Tin><<<grid, 256, 0, st>>>(vol + b * vox, p->pair_surf[b], g.nx, g.ny,
+                                                  g.nz); note_launch();
+    DTV_LAUNCH_CHECK();
+  }
+  return DTV_OK;
+}
+
 int forward_impl(Plan* p, const void* vol, int vol_dtype, int batch, float* out, int epilogue,
                  const float* g, float sigma, double* abs_sum, cudaStream_t st) {
   const GeomParams& gp = p->gp;
   int rc;
   const bool tex = (p->flags & DTV_PLAN_TEX) != 0;
+  const bool pairs = (p->flags & DTV_PLAN_TEX_PAIRS) != 0;
   switch (vol_dtype) {
     case DTV_F32:
-      rc = tex ? stage_volume_tex(p, (const float*)vol, batch, st)
-               : stage_volume_soft(p, (const float*)vol, batch, st);
+      rc = pairs ? stage_volume_pairs(p, (const float*)vol, batch, st)
+                 : tex ? stage_volume_tex(p, (const float*)vol, batch, st)
+                       : stage_volume_soft(p, (const float*)vol, batch, st);
       break;
     case DTV_F16:
-      rc = tex ? stage_volume_tex(p, (const __half*)vol, batch, st)
-               : stage_volume_soft(p, (const __half*)vol, batch, st);
+      rc = pairs ? stage_volume_pairs(p, (const __half*)vol, batch, st)
+                 : tex ? stage_volume_tex(p, (const __half*)vol, batch, st)
+                       : stage_volume_soft(p, (const __half*)vol, batch, st);
       break;
     default:
-      rc = tex ? stage_volume_tex(p, (const __nv_bfloat16*)vol, batch, st)
-               : stage_volume_soft(p, (const __nv_bfloat16*)vol, batch, st);
+      rc = pairs ? stage_volume_pairs(p, (const __nv_bfloat16*)vol, batch, st)
+                 : tex ? stage_volume_tex(p, (const __nv_bfloat16*)vol, batch, st)
+                       : stage_volume_soft(p, (const __nv_bfloat16*)vol, batch, st);
       break;
   }
   if (rc) return rc;
@@ -376,7 +454,9 @@ int forward_impl(Plan* p, const void* vol, int vol_dtype, int batch, float* out,
   FPOut o{out, g, sigma, abs_sum, epilogue};
   const int tiles = ((gp.nu + kTileU - 1) / kTileU) * ((gp.nv + kTileV - 1) / kTileV);
   dim3 grid(tiles, gp.n_views, batch);
-  if (tex) {
+  if (pairs) {
+    fp_pair_kernel<<<grid, kFPThreads, 0, st>>>(rp, p->d_fpv, p->pair_tex_dev, o); note_launch();
+  } else if (tex) {
     fp_tex_kernel<<<grid, kFPThreads, 0, st>>>(rp, p->d_fpv, p->vol_tex_dev, o); note_launch();
   } else if (p->stage_dtype == DTV_F16) {
     fp_soft_kernel<__half><<<grid, kFPThreads, 0, st>>>(rp, p->d_fpv, (const __half*)p->d_vol_pad,

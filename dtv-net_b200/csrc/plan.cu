@@ -32,6 +32,15 @@ void free_plan(Plan* p) {
       if (p->vol_surf[b]) cudaDestroySurfaceObject(p->vol_surf[b]);
   }
   free(p->vol_surf);
+  for (int b = 0; p->pair_arrays && b < p->max_batch; ++b) {
+    if (p->pair_tex && p->pair_tex[b]) cudaDestroyTextureObject(p->pair_tex[b]);
+    if (p->pair_surf && p->pair_surf[b]) cudaDestroySurfaceObject(p->pair_surf[b]);
+    if (p->pair_arrays[b]) cudaFreeArray(p->pair_arrays[b]);
+  }
+  free(p->pair_arrays);
+  free(p->pair_tex);
+  free(p->pair_surf);
+  cudaFree(p->pair_tex_dev);
   if (p->vol_arrays) {
     for (int b = 0; b < p->max_batch; ++b)
       if (p->vol_arrays[b]) cudaFreeArray(p->vol_arrays[b]);
@@ -71,7 +80,10 @@ int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Pla
   DTV_CHECK(out != nullptr, "out is NULL");
   *out = nullptr;
   DTV_CHECK(max_batch > 0, "max_batch must be positive");
-  DTV_CHECK((flags & ~(DTV_PLAN_TEX | DTV_PLAN_STAGE_F16)) == 0, "unknown plan flags 0x%x", flags);
+  DTV_CHECK((flags & ~(DTV_PLAN_TEX | DTV_PLAN_STAGE_F16 | DTV_PLAN_TEX_PAIRS)) == 0,
+            "unknown plan flags 0x%x", flags);
+  DTV_CHECK(!((flags & DTV_PLAN_TEX) && (flags & DTV_PLAN_TEX_PAIRS)),
+            "DTV_PLAN_TEX and DTV_PLAN_TEX_PAIRS are exclusive");
   int ndev = 0;
   DTV_CUDA_TRY(cudaGetDeviceCount(&ndev));
   DTV_CHECK(device >= 0 && device < ndev, "device %d out of range (%d devices)", device, ndev);
@@ -126,9 +138,7 @@ int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Pla
     p->vol_arrays = (cudaArray_t*)calloc(max_batch, sizeof(cudaArray_t));
     p->vol_tex = (cudaTextureObject_t*)calloc(max_batch, sizeof(cudaTextureObject_t));
     p->vol_surf = (cudaSurfaceObject_t*)calloc(max_batch, sizeof(cudaSurfaceObject_t));
-    p->sino_arrays = (cudaArray_t*)calloc(1, sizeof(cudaArray_t));
-    p->sino_tex = (cudaTextureObject_t*)calloc(1, sizeof(cudaTextureObject_t));
-    if (!p->vol_arrays || !p->vol_tex || !p->vol_surf || !p->sino_arrays || !p->sino_tex) {
+    if (!p->vol_arrays || !p->vol_tex || !p->vol_surf) {
       free_plan(p);
       return fail(DTV_ERR_ALLOC, "host allocation failed");
     }
@@ -151,21 +161,59 @@ int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Pla
     PLAN_CUDA(cudaMalloc(&p->vol_tex_dev, sizeof(cudaTextureObject_t) * max_batch));
     PLAN_CUDA(cudaMemcpy(p->vol_tex_dev, p->vol_tex, sizeof(cudaTextureObject_t) * max_batch,
                          cudaMemcpyHostToDevice));
-    int max_layers = 0;
+  }
+  int max_layers = 0;
+  if (flags & (DTV_PLAN_TEX | DTV_PLAN_TEX_PAIRS))
     PLAN_CUDA(cudaDeviceGetAttribute(&max_layers, cudaDevAttrMaxTexture2DLayeredLayers, device));
-    if (gp.n_views <= max_layers) {
-      cudaChannelFormatDesc sd = cudaCreateChannelDesc<float>();
-      PLAN_CUDA(cudaMalloc3DArray(&p->sino_arrays[0], &sd,
-                                  make_cudaExtent(gp.nu, gp.nv, gp.n_views), cudaArrayLayered));
-      rc = make_tex3d(p->sino_arrays[0], 1, &p->sino_tex[0]);
+  if (flags & DTV_PLAN_TEX_PAIRS) {
+    if (gp.nz + 3 > max_layers) {
+      free_plan(p);
+      return fail(DTV_ERR_UNSUPPORTED, "nz + 3 = %d exceeds the %d texture layers of the device",
+                  gp.nz + 3, max_layers);
+    }
+    p->pair_arrays = (cudaArray_t*)calloc(max_batch, sizeof(cudaArray_t));
+    p->pair_tex = (cudaTextureObject_t*)calloc(max_batch, sizeof(cudaTextureObject_t));
+    p->pair_surf = (cudaSurfaceObject_t*)calloc(max_batch, sizeof(cudaSurfaceObject_t));
+    if (!p->pair_arrays || !p->pair_tex || !p->pair_surf) {
+      free_plan(p);
+      return fail(DTV_ERR_ALLOC, "host allocation failed");
+    }
+    cudaChannelFormatDesc cd = cudaCreateChannelDescHalf2();
+    for (int b = 0; b < max_batch; ++b) {
+      PLAN_CUDA(cudaMalloc3DArray(&p->pair_arrays[b], &cd,
+                                  make_cudaExtent(gp.nx, gp.ny, gp.nz + 3),
+                                  cudaArrayLayered | cudaArraySurfaceLoadStore));
+      rc = make_tex3d(p->pair_arrays[b], 1, &p->pair_tex[b]);
       if (rc) {
         free_plan(p);
         return rc;
       }
-    } else {
-      // more views than layers: the backprojector samples in software
-      free(p->sino_tex);
-      p->sino_tex = nullptr;
+      cudaResourceDesc rd;
+      memset(&rd, 0, sizeof(rd));
+      rd.resType = cudaResourceTypeArray;
+      rd.res.array.array = p->pair_arrays[b];
+      PLAN_CUDA(cudaCreateSurfaceObject(&p->pair_surf[b], &rd));
+    }
+    PLAN_CUDA(cudaMalloc(&p->pair_tex_dev, sizeof(cudaTextureObject_t) * max_batch));
+    PLAN_CUDA(cudaMemcpy(p->pair_tex_dev, p->pair_tex, sizeof(cudaTextureObject_t) * max_batch,
+                         cudaMemcpyHostToDevice));
+  }
+  if ((flags & (DTV_PLAN_TEX | DTV_PLAN_TEX_PAIRS)) && gp.n_views <= max_layers) {
+    // backprojector: the sinogram as a layered texture (one layer per view);
+    // with more views than layers the backprojector samples in software
+    p->sino_arrays = (cudaArray_t*)calloc(1, sizeof(cudaArray_t));
+    p->sino_tex = (cudaTextureObject_t*)calloc(1, sizeof(cudaTextureObject_t));
+    if (!p->sino_arrays || !p->sino_tex) {
+      free_plan(p);
+      return fail(DTV_ERR_ALLOC, "host allocation failed");
+    }
+    cudaChannelFormatDesc sd = cudaCreateChannelDesc<float>();
+    PLAN_CUDA(cudaMalloc3DArray(&p->sino_arrays[0], &sd, make_cudaExtent(gp.nu, gp.nv, gp.n_views),
+                                cudaArrayLayered));
+    rc = make_tex3d(p->sino_arrays[0], 1, &p->sino_tex[0]);
+    if (rc) {
+      free_plan(p);
+      return rc;
     }
   }
 #undef PLAN_CUDA

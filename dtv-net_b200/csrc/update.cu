@@ -565,7 +565,7 @@ __device__ __forceinline__ float clipf(float x, float m) { return copysignf(fmin
 // The duals are clipped in place; neighbours may read a value before or after
 // its clip, and clipping is idempotent, so both give the same result.
 template <class T>
-__global__ void __launch_bounds__(256) pdhg_primal_kernel(T* __restrict__ f, T* __restrict__ fbar,
+__global__ void __launch_bounds__(256) pdhg_primal_kernel(float* __restrict__ f, T* __restrict__ fbar,
                                                           const float* __restrict__ recon, float* p,
                                                           float* q, float* s,
                                                           const float* __restrict__ c, Dims d,
@@ -594,10 +594,10 @@ __global__ void __launch_bounds__(256) pdhg_primal_kernel(T* __restrict__ f, T* 
     sprev = ss;
     const int64_t t = cl.base + i;
     const float reg = fmaf(v0, dx, fmaf(v1, dy, fmaf(v2, dz, mu * c[t])));
-    const float fo = load_as_float(f, t);
+    const float fo = f[t];
     const float fn = fo - recon[t] - tau * reg;
     store_from_float(fbar, t, 2.f * fn - fo);
-    store_from_float(f, t, fn);
+    f[t] = fn;
   }
 }
 
@@ -846,7 +846,7 @@ int dtv_pdhg_dual(const void* fbar, float* p, float* q, float* s, float* c, cons
   return DTV_OK;
 }
 
-int dtv_pdhg_primal(void* f, void* fbar, const float* recon, float* p, float* q, float* s,
+int dtv_pdhg_primal(float* f, void* fbar, const float* recon, float* p, float* q, float* s,
                     const float* c, const int32_t size[3], int32_t batch,
                     const dtv_pdhg_params* prm, const void* ws, void* stream) {
   DTV_CHECK(f && fbar && recon && p && q && s && c && size && prm && ws, "NULL argument");
@@ -857,11 +857,11 @@ int dtv_pdhg_primal(void* f, void* fbar, const float* recon, float* p, float* q,
   const L1Chan* ch = reinterpret_cast<const L1Chan*>(ws);
   if (prm->f_dtype == DTV_F32) {
     pdhg_primal_kernel<float><<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(
-        (float*)f, (float*)fbar, recon, p, q, s, c, d, prm->tau, prm->mu, prm->v[0], prm->v[1],
+        f, (float*)fbar, recon, p, q, s, c, d, prm->tau, prm->mu, prm->v[0], prm->v[1],
         prm->v[2], ch); note_launch();
   } else {
     pdhg_primal_kernel<__half><<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(
-        (__half*)f, (__half*)fbar, recon, p, q, s, c, d, prm->tau, prm->mu, prm->v[0], prm->v[1],
+        f, (__half*)fbar, recon, p, q, s, c, d, prm->tau, prm->mu, prm->v[0], prm->v[1],
         prm->v[2], ch); note_launch();
   }
   DTV_LAUNCH_CHECK();

@@ -81,7 +81,9 @@ class DTVCP(_Graphable):
     recon = BP(w) (:40); dual ascent + L1-ball projections + non-negativity dual
     in one fused pass plus an exact device-side threshold search (:41-47);
     primal step and over-relaxation in one fused pass (:48-54).
-    ``f_dtype`` torch.float16 stores f and fbar in FP16 (FP32 arithmetic).
+    ``f_dtype`` torch.float16 stores fbar, the projector input, in FP16; the
+    iterate f and all arithmetic stay FP32 (rounding f itself each iteration
+    would drop updates below its FP16 resolution).
     """
 
     def __init__(self, plan: Plan, cascades: int = 30, sigma: float = 1e-7, tau: float = 1e-7,
@@ -129,7 +131,7 @@ class DTVCP(_Graphable):
         b = image.numel() // int(np.prod(plan.vol_shape(1)))
         st = {
             "b": b,
-            "f": torch.empty(vs, dtype=self.f_dtype, device=dev),
+            "f": torch.empty(vs, dtype=torch.float32, device=dev),
             "fbar": torch.empty(vs, dtype=self.f_dtype, device=dev),
             "p": torch.zeros(vs, dtype=torch.float32, device=dev),
             "q": torch.zeros(vs, dtype=torch.float32, device=dev),
@@ -160,7 +162,7 @@ class DTVCP(_Graphable):
         for it in range(self.cascades):
             if it % self.t_refresh == 0:
                 st["t"].zero_()
-                call("dtv_diff_abs_sums", _ptr(f), prm.f_dtype, size, b, prm.quirk,
+                call("dtv_diff_abs_sums", _ptr(f), _lib.DTV_F32, size, b, prm.quirk,
                      _ptr(st["t"]), stream)
             plan.forward(fbar, out=st["w"], epilogue=_lib.DTV_EPI_PDHG, g=st["g"],
                          sigma=self.sigma, abs_sum=st["loss"][it:it + 1])

@@ -133,13 +133,16 @@ def check_input(t: torch.Tensor, name: str, shape=None, dtypes=(torch.float32,))
 class Plan:
     """A geometry uploaded to one GPU with sampler staging for ``max_batch``
     volumes. ``sampler``: "soft" (software trilinear, FP32 weights; required
-    for the exact adjoint) or "tex" (hardware texture filtering, like the
-    reference). ``stage_f16`` stages projected volumes as FP16."""
+    for the exact adjoint), "tex" (hardware trilinear texture filtering, like
+    the reference) or "pairs" (FP16 z-plane pairs in a layered texture: one
+    bilinear fetch per sample, z interpolated in FP32). The backprojector
+    samples the sinogram through a texture for "tex" and "pairs".
+    ``stage_f16`` stages projected volumes as FP16 ("soft"/"tex")."""
 
     def __init__(self, geometry: Geometry, max_batch: int = 1, sampler: str = "soft",
                  stage_f16: bool = False, device=None):
-        if sampler not in ("soft", "tex"):
-            raise ValueError("sampler must be 'soft' or 'tex'")
+        if sampler not in ("soft", "tex", "pairs"):
+            raise ValueError("sampler must be 'soft', 'tex' or 'pairs'")
         dev = torch.device("cuda", torch.cuda.current_device()) if device is None else \
             torch.device(device)
         if dev.type != "cuda":
@@ -150,8 +153,8 @@ class Plan:
         self.max_batch = int(max_batch)
         self.sampler = sampler
         self.stage_f16 = bool(stage_f16)
-        flags = (_lib.DTV_PLAN_TEX if sampler == "tex" else 0) | \
-                (_lib.DTV_PLAN_STAGE_F16 if stage_f16 else 0)
+        flags = {"soft": 0, "tex": _lib.DTV_PLAN_TEX, "pairs": _lib.DTV_PLAN_TEX_PAIRS}[sampler] | \
+            (_lib.DTV_PLAN_STAGE_F16 if stage_f16 else 0)
         h = ctypes.c_void_p()
         call("dtv_plan_create", ctypes.byref(geometry.struct), self.max_batch, flags,
              self.device.index, ctypes.byref(h))

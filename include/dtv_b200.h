@@ -64,6 +64,11 @@ extern "C" {
 #define DTV_PLAN_SOFT 0x0      /* software trilinear/bilinear, FP32 weights (default) */
 #define DTV_PLAN_TEX 0x1       /* hardware texture filtering (8-bit fraction weights) */
 #define DTV_PLAN_STAGE_F16 0x2 /* stage the projected volume as FP16 (soft sampler)  */
+/* Forward projector through a 2-D layered FP16 texture whose texel (x, y, L)
+ * holds the z pair (f[L-2], f[L-1]): one bilinear fetch (8-bit x/y weights)
+ * returns both planes and the z interpolation is done in FP32. Backprojector
+ * as DTV_PLAN_TEX. Needs nz + 3 <= the device's layered-texture layer limit. */
+#define DTV_PLAN_TEX_PAIRS 0x4
 
 /* ---- forward-projector epilogues ---------------------------------------- */
 #define DTV_EPI_STORE 0    /* out = FP(vol)                                        */
@@ -245,7 +250,8 @@ typedef struct dtv_pdhg_params {
   float mu;     /* non-negativity weight (DTVCP.py:22)        */
   float v[3];   /* per-direction weights v1,v2,v3 (:19-21)   */
   int32_t quirk; /* reference D_y wrap (Gradients.py:18-25)   */
-  int32_t f_dtype; /* storage of f and fbar: DTV_F32 or DTV_F16 */
+  int32_t f_dtype; /* storage of fbar, the projector input: DTV_F32 or DTV_F16
+                      (f itself is always FP32) */
 } dtv_pdhg_params;
 
 /* Workspace bytes of the fused dual step (three L1-ball channels). */
@@ -261,7 +267,7 @@ DTV_API int dtv_pdhg_dual(const void* fbar, float* p, float* q, float* s, float*
  * thresholds found by dtv_pdhg_dual), fnew = f - recon - tau*(v1 D_x^T p +
  * v2 D_y^T q + v3 D_z^T s + mu c), fbar = 2 fnew - f, f = fnew.
  * (DTVCP.py:44-54) */
-DTV_API int dtv_pdhg_primal(void* f, void* fbar, const float* recon, float* p, float* q, float* s,
+DTV_API int dtv_pdhg_primal(float* f, void* fbar, const float* recon, float* p, float* q, float* s,
                     const float* c, const int32_t size[3], int32_t batch,
                     const dtv_pdhg_params* prm, const void* workspace, void* stream);
 

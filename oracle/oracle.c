@@ -16,7 +16,8 @@
  * value 0 in unnormalised texel coordinates (the reference's texture setup,
  * Standard/plug/kernel/forwardKernel.cu:102-107). With tex_quant != 0 the
  * interpolation weights are rounded to 1/256, the 8-bit fraction the CUDA
- * programming guide documents for hardware linear filtering.
+ * programming guide documents for hardware linear filtering; tex_quant == 2
+ * rounds only the x/y weights (bilinear hardware filtering of z-plane pairs).
  *
  * Parity pin: the literal layer is compared against the reference kernels
  * themselves (built from their unmodified sources, run on a GPU) through the
@@ -59,7 +60,8 @@ static double tri(const double* v, int nx, int ny, int nz, double x, double y, d
   double fx = floor(x), fy = floor(y), fz = floor(z);
   if (fx < -1.0 || fy < -1.0 || fz < -1.0 || fx > nx || fy > ny || fz > nz) return 0.0;
   int ix = (int)fx, iy = (int)fy, iz = (int)fz;
-  double ax = qw(x - fx, q), ay = qw(y - fy, q), az = qw(z - fz, q);
+  /* q == 2: x/y weights at 1/256, z weight exact (the z-pair sampler) */
+  double ax = qw(x - fx, q), ay = qw(y - fy, q), az = qw(z - fz, q == 1);
   double acc = 0.0;
   for (int dz = 0; dz < 2; ++dz) {
     int zz = iz + dz;

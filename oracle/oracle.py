@@ -179,7 +179,9 @@ def _as_batch(x: np.ndarray, shape3):
     return x.reshape((b,) + tuple(shape3)), b
 
 
-def forward(geo: Geometry, vol, q: bool = False) -> np.ndarray:
+def forward(geo: Geometry, vol, q: int = 0) -> np.ndarray:
+    """q: 0 exact weights, 1 all weights at 1/256 (3-D texture filtering),
+    2 x/y weights at 1/256 and exact z (z-pair layered texture)."""
     v, b = _as_batch(vol, geo.vol_shape)
     out = np.empty((b,) + geo.sino_shape)
     lib().oracle_forward(ctypes.byref(geo.og), _p(geo.views), _p(v), b, int(q), _p(out))

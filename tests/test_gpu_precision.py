@@ -1,0 +1,106 @@
+"""Precision gates against the FP64 oracle (relative RMSE <= 1e-3 for every
+projection and reconstruction mode), on a reduced copy of the sparse-view DTV
+configuration, plus size-independent properties at the full configuration
+(256^3, 64 views of 384^2 at 1.2 mm)."""
+import numpy as np
+import pytest
+import torch
+
+import dtvb200
+import oracle as O
+from dtvb200.phantom import ellipsoids
+from helpers import rel_rmse
+
+pytestmark = pytest.mark.gpu
+
+GATE = 1e-3  # relative RMSE against FP64
+
+
+def reduced(cuda, n=48, views=12):
+    nd = int(n * 1.5)
+    ang = np.linspace(0, 360, views, endpoint=False)
+    args = (ang, (n, n, n), (1.0, 1.0, 1.0), (nd, nd), (1.2, 1.2), 500.0, 1000.0)
+    geo = dtvb200.circular(*args)
+    og = O.circular_geometry(*args)
+    truth = ellipsoids((n, n, n), seed=3).numpy()
+    return geo, og, truth
+
+
+@pytest.mark.parametrize("sampler", ["soft", "tex", "pairs"])
+def test_projection_gate(cuda, sampler):
+    geo, og, truth = reduced(cuda)
+    plan = dtvb200.Plan(geo, sampler=sampler, device=cuda)
+    out = plan.forward(torch.from_numpy(truth).to(cuda)).cpu().numpy()
+    ref = O.forward(og, truth).reshape(out.shape)
+    assert rel_rmse(out, ref) < GATE
+    sino = ref.astype(np.float32)
+    bp = plan.backward(torch.from_numpy(sino).to(cuda)).cpu().numpy()
+    assert rel_rmse(bp, O.backward(og, sino).reshape(bp.shape)) < GATE
+
+
+@pytest.mark.parametrize("sampler,fdt", [("soft", torch.float32), ("tex", torch.float32),
+                                         ("pairs", torch.float32), ("tex", torch.float16),
+                                         ("pairs", torch.float16)])
+def test_dtv_reconstruction_gate(cuda, sampler, fdt):
+    geo, og, truth = reduced(cuda)
+    sino = O.forward(og, truth).reshape(1, 1, *og.sino_shape)
+    iters, sigma = 15, 2e-3
+    prm = dict(sigma=sigma, tau=sigma, mu=1.0, v=(0.5, 0.5, 0.5), quirk=False)
+    fp = lambda x: O.forward(og, x).reshape(x.shape[0], 1, *og.sino_shape)  # noqa: E731
+    bp = lambda s: O.backward(og, s).reshape(s.shape[0], 1, *og.vol_shape)  # noqa: E731
+    ref = O.dtvcp_run(fp, bp, np.zeros((1, 1) + og.vol_shape), sino, geo.volume_size, iters,
+                      sigma, sigma, 1.0, (0.5, 0.5, 0.5), quirk=False)
+    plan = dtvb200.Plan(geo, sampler=sampler, device=cuda)
+    alg = dtvb200.DTVCP(plan, iters, f_dtype=fdt, use_graph=True, **prm)
+    f = alg.run(torch.zeros(plan.vol_shape(1), device=cuda),
+                torch.from_numpy(sino.astype(np.float32)).to(cuda)).cpu().numpy()
+    assert float(np.abs(ref).max()) > 0
+    assert rel_rmse(f, ref) < GATE
+
+
+@pytest.fixture(scope="module")
+def full(cuda):
+    n, nd = 256, 384
+    ang = np.linspace(0, 360, 64, endpoint=False)
+    geo = dtvb200.circular(ang, (n, n, n), (1.0,) * 3, (nd, nd), (1.2, 1.2), 500.0, 1000.0)
+    x = ellipsoids((n, n, n), seed=7, device=cuda)
+    return geo, x
+
+
+def test_full_size_linearity_and_samplers(cuda, full):
+    geo, x = full
+    soft = dtvb200.Plan(geo, sampler="soft", device=cuda)
+    y = torch.rand_like(x)
+    a, b = 0.7, -1.3
+    lhs = soft.forward(a * x + b * y)
+    rhs = a * soft.forward(x) + b * soft.forward(y)
+    assert float(((lhs - rhs).double() ** 2).mean().sqrt() / (rhs.double() ** 2).mean().sqrt()) < 1e-5
+    ref = soft.forward(x).double()
+    for sampler in ("tex", "pairs"):
+        out = dtvb200.Plan(geo, sampler=sampler, device=cuda).forward(x).double()
+        assert float(((out - ref) ** 2).mean().sqrt() / (ref ** 2).mean().sqrt()) < GATE
+
+
+def test_full_size_adjoint_dot_test(cuda, full):
+    geo, x = full
+    soft = dtvb200.Plan(geo, sampler="soft", device=cuda)
+    g = torch.Generator(device=cuda).manual_seed(3)
+    y = torch.rand(soft.sino_shape(1), device=cuda, generator=g)
+    lhs = float((soft.forward(x).double() * y.double()).sum())
+    rhs = float((x.double() * soft.adjoint(y).double()).sum())
+    assert abs(lhs - rhs) / abs(lhs) < 1e-5
+
+
+def test_full_size_chords_of_a_uniform_volume(cuda, full):
+    """FP of the all-ones volume is each ray's chord length through the box
+    (to within one sample step)."""
+    geo, x = full
+    soft = dtvb200.Plan(geo, sampler="soft", device=cuda)
+    ones = torch.ones_like(x)
+    s = soft.forward(ones)
+    assert float(s.max()) <= 256 * np.sqrt(3) + 1.0
+    assert float(s.max()) >= 256.0
+    # the central ray of view 0 crosses 256 voxels
+    nd = 384
+    centre = s[0, 0, 0, nd // 2 - 1:nd // 2 + 1, nd // 2 - 1:nd // 2 + 1]
+    assert torch.all((centre - 256.0).abs() < 2.0)

@@ -76,7 +76,19 @@ def test_forward_tex_matches_oracle_tex_mode(cuda, kind):
 
 
 @pytest.mark.parametrize("kind", KINDS)
-@pytest.mark.parametrize("sampler", ["soft", "tex"])
+def test_forward_pairs_matches_oracle(cuda, kind):
+    """z-pair sampler: FP16 planes, 1/256 x/y weights, exact z weights."""
+    g, og = make_case(kind)
+    plan = dtvb200.Plan(g, max_batch=2, sampler="pairs", device=cuda)
+    vol = blob_volume(np.random.default_rng(21), og.vol_shape, 2)
+    v16 = vol.astype(np.float16).astype(np.float32)
+    out = plan.forward(to_dev(vol, cuda)).cpu().numpy()
+    assert rel_rmse(out, O.forward(og, v16, q=2).reshape(out.shape)) < 5e-4
+    assert rel_rmse(out, O.forward(og, vol).reshape(out.shape)) < 1e-3
+
+
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("sampler", ["soft", "tex", "pairs"])
 def test_backward_fdk_matches_oracle(cuda, kind, sampler):
     g, og = make_case(kind)
     plan = dtvb200.Plan(g, max_batch=2, sampler=sampler, device=cuda)
@@ -87,7 +99,7 @@ def test_backward_fdk_matches_oracle(cuda, kind, sampler):
         ref = O.backward(og, sino).reshape(out.shape)
         assert rel_rmse(out, ref) < 1e-5
         assert rel_max(out, ref) < 1e-4
-    else:
+    else:  # "tex" and "pairs" sample the sinogram through the same texture
         ref = O.backward(og, sino, q=True).reshape(out.shape)
         assert rel_rmse(out, ref) < 5e-4
 
@@ -209,7 +221,7 @@ def _ref_proj():
 
 
 @pytest.mark.parametrize("name", ["s1", "s2", "s3"])
-@pytest.mark.parametrize("sampler", ["soft", "tex"])
+@pytest.mark.parametrize("sampler", ["soft", "tex", "pairs"])
 def test_matches_reference_kernels_standard(cuda, name, sampler):
     """Through the drop-in module with the reference's argument list."""
     z = _ref_proj()
@@ -226,12 +238,14 @@ def test_matches_reference_kernels_standard(cuda, name, sampler):
     finally:
         J._SAMPLER, J._plans = old, {}
     assert fp.shape == z[f"{name}_fp"].shape and bp.shape == z[f"{name}_bp"].shape
-    tol = 5e-4 if sampler == "tex" else 5e-3  # the reference filters with 1/256 weights
+    # the reference filters with 1/256 weights in float32 coordinates; "pairs"
+    # also rounds the volume to FP16
+    tol = {"tex": 5e-4, "soft": 5e-3, "pairs": 2e-3}[sampler]
     assert rel_rmse(fp.cpu().numpy(), z[f"{name}_fp"]) < tol
     assert rel_rmse(bp.cpu().numpy(), z[f"{name}_bp"]) < tol
 
 
-@pytest.mark.parametrize("sampler", ["soft", "tex"])
+@pytest.mark.parametrize("sampler", ["soft", "tex", "pairs"])
 def test_matches_reference_kernels_vector(cuda, sampler):
     z = _ref_proj()
     import JITBeijingGeometry as J
@@ -246,7 +260,7 @@ def test_matches_reference_kernels_vector(cuda, sampler):
         bp = J.backward(to_dev(z["v_sino_in"], cuda), vs, ds, pv, 0)
     finally:
         JITBeijingGeometry._SAMPLER, J._plans = JS._SAMPLER, {}
-    tol = 5e-4 if sampler == "tex" else 5e-3
+    tol = {"tex": 5e-4, "soft": 5e-3, "pairs": 2e-3}[sampler]
     assert rel_rmse(fp.cpu().numpy(), z["v_fp"]) < tol
     assert rel_rmse(bp.cpu().numpy(), z["v_bp"]) < tol
 
