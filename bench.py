@@ -34,6 +34,11 @@ UNIT = "GRay·samples/s"
 CFG = dict(nx=256, ny=256, nz=256, voxel=1.0, nu=384, nv=384, pitch=1.2, n_views=64,
            sod=500.0, sdd=1000.0, iters=100, i0=1e5, seed=2024)
 
+# DRAM traffic of one forward-projector launch on this workload
+# (dram__bytes_read.sum + dram__bytes_write.sum, one ncu --set full capture of
+# `python bench.py --profile 12`) and that capture's texture-pipe utilisation.
+FP_NCU = {"pairs": {"traffic": 274.856448e6 + 61.563648e6, "tex_pipe_pct": 94.2}}
+
 
 def workload_name(c):
     return (f"sparse-view DTV: {c['nx']}^3 x {c['voxel']:g} mm, {c['n_views']} views/360deg, "
@@ -389,7 +394,9 @@ def run_ours(args):
         "samples_per_recon": units,
         "per_iteration_ms": {"forward": t_fp, "backward": t_bp, "updates": t_up},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved / hbm_peak, "traffic": None,
+                     "frac": achieved / hbm_peak,
+                     "traffic": FP_NCU.get(args.sampler, {}).get("traffic"),
+                     "texture_pipe_pct_of_peak": FP_NCU.get(args.sampler, {}).get("tex_pipe_pct"),
                      "kernel": "forward projector (staging + ray kernel)",
                      "algorithmic_bytes_per_launch": fp_bytes,
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
@@ -408,6 +415,30 @@ def run_ours(args):
     return 0
 
 
+def run_profile(args):
+    """N eager iterations of the workload (for ncu): forward projector,
+    backprojector and fused updates, one launch each per iteration."""
+    import torch
+
+    import dtvb200
+    from dtvb200.phantom import poisson_noise
+    dev = torch.device("cuda", 0)
+    c = dict(CFG)
+    if args.small:
+        c.update(nx=64, ny=64, nz=64, nu=96, nv=96, n_views=16)
+    geo, truth, _ = make_problem(dev, c, c["seed"])
+    plan = dtvb200.Plan(geo, max_batch=1, sampler=args.sampler, device=dev)
+    sino = poisson_noise(plan.forward(truth), c["i0"], seed=c["seed"])
+    prm = dtv_params(plan, dev)
+    alg = dtvb200.DTVCP(plan, args.profile, t_refresh=10, use_graph=False, **prm)
+    f = alg.run(torch.zeros(plan.vol_shape(1), device=dev), sino)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_iterations": args.profile, "sampler": args.sampler,
+                      "loss_first_last": [float(alg.losses[0]), float(alg.losses[-1])],
+                      "f_abs_sum": float(f.abs().sum())}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -418,11 +449,15 @@ def main():
     ap.add_argument("--small", action="store_true", help="64^3 smoke-size workload")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile", type=int, default=0, metavar="N",
+                    help="profiling run: N eager DTV iterations of the workload, no timing")
     args = ap.parse_args()
     if args.warmup < 3 and not args.small:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile:
+        return run_profile(args)
     return run_ours(args)
 
 

@@ -114,8 +114,6 @@ struct Plan {
   int64_t pad_elems;  // elements of one padded volume
   // soft bilinear staging: zero-padded sinogram of one batch item
   float* d_sino_pad;
-  // adjoint accumulator: one padded FP32 volume
-  float* d_adj_pad;
   // texture sampler (DTV_PLAN_TEX): one 3-D array per batch item for the
   // volume, one layered array for a sinogram
   cudaArray_t* vol_arrays;

@@ -470,71 +470,133 @@ int forward_impl(Plan* p, const void* vol, int vol_dtype, int batch, float* out,
 }
 
 // ---- exact transpose of the soft forward projector -------------------------------------
-__global__ void __launch_bounds__(kFPThreads) adjoint_kernel(RayParams rp, const FPView* __restrict__ views,
-                                                             const float* __restrict__ sino,
-                                                             float* __restrict__ acc_pad, int b) {
-  const int tiles_u = (rp.nu + kTileU - 1) / kTileU;
-  int u, v;
-  tile_pixel(tiles_u, u, v);
-  const int n = blockIdx.y;
-  if (u >= rp.nu || v >= rp.nv) return;
-  const float y =
-      sino[((int64_t)b * rp.n_views + n) * rp.nu * rp.nv + (int64_t)v * rp.nu + u] * rp.scale;
-  if (y == 0.f) return;
-  const RaySetup rs = setup_ray(rp, views[n], u, v);
-  const int px = rp.nx + 2 * kPad, pxy = px * (rp.ny + 2 * kPad);
-  const float mx = (float)rp.nx, my = (float)rp.ny, mz = (float)rp.nz;
-  for (int k = 0; k < rs.count; ++k) {
-    const float kf = (float)k;
-    const float x = fmaf(kf, rs.dp[0], rs.p0[0]), yy = fmaf(kf, rs.dp[1], rs.p0[1]),
-                z = fmaf(kf, rs.dp[2], rs.p0[2]);
-    const float fx = floorf(x), fy = floorf(yy), fz = floorf(z);
-    const float ax = x - fx, ay = yy - fy, az = z - fz;
-    const int ix = (int)fminf(fmaxf(fx, -2.f), mx) + kPad;
-    const int iy = (int)fminf(fmaxf(fy, -2.f), my) + kPad;
-    const int iz = (int)fminf(fmaxf(fz, -2.f), mz) + kPad;
-    float* base = acc_pad + (iz * pxy + iy * px + ix);
-    // weights in the same form as the forward lerps: v0 + a(v1 - v0)
-    const float wz1 = az * y, wz0 = y - wz1;
-    const float w00 = wz0 - ay * wz0, w01 = ay * wz0, w10 = wz1 - ay * wz1, w11 = ay * wz1;
-    atomicAdd(base, w00 - ax * w00);
-    atomicAdd(base + 1, ax * w00);
-    atomicAdd(base + px, w01 - ax * w01);
-    atomicAdd(base + px + 1, ax * w01);
-    atomicAdd(base + pxy, w10 - ax * w10);
-    atomicAdd(base + pxy + 1, ax * w10);
-    atomicAdd(base + pxy + px, w11 - ax * w11);
-    atomicAdd(base + pxy + px + 1, ax * w11);
-  }
-}
+// A^T y scatters every forward sample's value y_r * scale * w_tap onto its 8
+// trilinear taps. Instead of 8 global atomics per sample, the volume is cut
+// into kAB^3 bricks: one block owns a brick (plus a one-voxel halo) in shared
+// memory and, for every view, visits the rays that can reach it -- the
+// detector rectangle onto which the brick's box projects, through the view's
+// projective map -- rebuilding each ray with the forward projector's own
+// set-up and scattering only the samples whose base voxel floor(p) lies in the
+// brick (the first brick along an axis also takes base -1, whose upper taps
+// are inside). Every contributing sample belongs to exactly one brick, so the
+// sum is the exact transpose; each brick then adds its tile to the output once.
+constexpr int kAB = 16;         // brick edge (voxels)
+constexpr int kAT = kAB + 2;    // tile edge: voxels lo-1 .. lo+kAB
+constexpr int kAdjThreads = 256;
 
-__global__ void unpad_kernel(const float* __restrict__ pad, float* __restrict__ out, int nx, int ny,
-                             int nz) {
-  const int64_t vol = (int64_t)nx * ny * nz;
-  const int px = nx + 2 * kPad, pxy = px * (ny + 2 * kPad);
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < vol;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int x = (int)(i % nx);
-    const int64_t r = i / nx;
-    const int y = (int)(r % ny), z = (int)(r / ny);
-    out[i] = pad[(int64_t)(z + kPad) * pxy + (y + kPad) * px + x + kPad];
+__global__ void __launch_bounds__(kAdjThreads) adjoint_brick_kernel(
+    RayParams rp, const FPView* __restrict__ views, const BPView* __restrict__ pviews,
+    const float* __restrict__ sino, float* __restrict__ out) {
+  __shared__ float tile[kAT * kAT * kAT];
+  const int nbx = (rp.nx + kAB - 1) / kAB, nby = (rp.ny + kAB - 1) / kAB;
+  const int bid = blockIdx.x;
+  const int lo[3] = {(bid % nbx) * kAB, ((bid / nbx) % nby) * kAB, (bid / (nbx * nby)) * kAB};
+  const int n3[3] = {rp.nx, rp.ny, rp.nz};
+  const int b = blockIdx.y;
+  for (int i = threadIdx.x; i < kAT * kAT * kAT; i += blockDim.x) tile[i] = 0.f;
+  // base voxels owned by this brick: [blo, bhi] per axis
+  float blo[3], bhi[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    blo[c] = lo[c] == 0 ? -1.f : (float)lo[c];
+    bhi[c] = (float)(min(lo[c] + kAB, n3[c]) - 1);
+  }
+  __syncthreads();
+  const int64_t per_view = (int64_t)rp.nu * rp.nv;
+  const float* sb = sino + (int64_t)b * rp.n_views * per_view;
+  for (int n = 0; n < rp.n_views; ++n) {
+    // detector rectangle of the box [blo, bhi + 1] through view n
+    const float* m = pviews[n].m;
+    float umin = 3.4e38f, umax = -3.4e38f, vmin = 3.4e38f, vmax = -3.4e38f;
+#pragma unroll
+    for (int cr = 0; cr < 8; ++cr) {
+      const float x = (cr & 1) ? bhi[0] + 1.f : blo[0];
+      const float y = (cr & 2) ? bhi[1] + 1.f : blo[1];
+      const float z = (cr & 4) ? bhi[2] + 1.f : blo[2];
+      const float h = fmaf(m[8], x, fmaf(m[9], y, fmaf(m[10], z, m[11])));
+      const float u = fmaf(m[0], x, fmaf(m[1], y, fmaf(m[2], z, m[3]))) / h;
+      const float v = fmaf(m[4], x, fmaf(m[5], y, fmaf(m[6], z, m[7]))) / h;
+      umin = fminf(umin, u); umax = fmaxf(umax, u);
+      vmin = fminf(vmin, v); vmax = fmaxf(vmax, v);
+    }
+    const int u0 = max(0, (int)fmaxf(floorf(umin) - 1.f, -1.f));
+    const int u1 = min(rp.nu - 1, (int)fminf(ceilf(umax) + 1.f, (float)rp.nu));
+    const int v0 = max(0, (int)fmaxf(floorf(vmin) - 1.f, -1.f));
+    const int v1 = min(rp.nv - 1, (int)fminf(ceilf(vmax) + 1.f, (float)rp.nv));
+    if (u0 > u1 || v0 > v1) continue;
+    const int w = u1 - u0 + 1;
+    const int cnt = w * (v1 - v0 + 1);
+    const FPView& f = views[n];
+    const float* sv = sb + n * per_view;
+    for (int r = threadIdx.x; r < cnt; r += blockDim.x) {
+      const int u = u0 + r % w, v = v0 + r / w;
+      const float y = __ldg(sv + (int64_t)v * rp.nu + u) * rp.scale;
+      if (y == 0.f) continue;
+      const RaySetup rs = setup_ray(rp, f, u, v);
+      if (rs.count <= 0) continue;
+      // samples that can have their base in this brick (one-sample margin)
+      float kl = 0.f, kh = (float)rs.count;
+      bool miss = false;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        if (rs.dp[c] != 0.f) {
+          const float ka = (blo[c] - 1.f - rs.p0[c]) / rs.dp[c];
+          const float kb = (bhi[c] + 2.f - rs.p0[c]) / rs.dp[c];
+          kl = fmaxf(kl, fminf(ka, kb));
+          kh = fminf(kh, fmaxf(ka, kb));
+        } else if (rs.p0[c] < blo[c] - 1.f || rs.p0[c] >= bhi[c] + 2.f) {
+          miss = true;
+        }
+      }
+      if (miss) continue;
+      const int k0 = max(0, (int)floorf(kl) - 1);
+      const int k1 = min(rs.count, (int)ceilf(kh) + 1);
+      for (int k = k0; k < k1; ++k) {
+        const float kf = (float)k;  // positions exactly as the forward projector forms them
+        const float x = fmaf(kf, rs.dp[0], rs.p0[0]), yy = fmaf(kf, rs.dp[1], rs.p0[1]),
+                    z = fmaf(kf, rs.dp[2], rs.p0[2]);
+        const float fx = floorf(x), fy = floorf(yy), fz = floorf(z);
+        if (fx < blo[0] || fx > bhi[0] || fy < blo[1] || fy > bhi[1] || fz < blo[2] ||
+            fz > bhi[2])
+          continue;
+        const float ax = x - fx, ay = yy - fy, az = z - fz;
+        const int tx = (int)fx - lo[0] + 1, ty = (int)fy - lo[1] + 1, tz = (int)fz - lo[2] + 1;
+        float* t = tile + (tz * kAT + ty) * kAT + tx;
+        const float wz1 = az * y, wz0 = y - wz1;
+        const float w00 = wz0 - ay * wz0, w01 = ay * wz0, w10 = wz1 - ay * wz1, w11 = ay * wz1;
+        atomicAdd(t, w00 - ax * w00);
+        atomicAdd(t + 1, ax * w00);
+        atomicAdd(t + kAT, w01 - ax * w01);
+        atomicAdd(t + kAT + 1, ax * w01);
+        atomicAdd(t + kAT * kAT, w10 - ax * w10);
+        atomicAdd(t + kAT * kAT + 1, ax * w10);
+        atomicAdd(t + kAT * kAT + kAT, w11 - ax * w11);
+        atomicAdd(t + kAT * kAT + kAT + 1, ax * w11);
+      }
+    }
+  }
+  __syncthreads();
+  float* ob = out + (int64_t)b * rp.nx * rp.ny * rp.nz;
+  for (int i = threadIdx.x; i < kAT * kAT * kAT; i += blockDim.x) {
+    const float val = tile[i];
+    if (val == 0.f) continue;
+    const int tx = i % kAT, ty = (i / kAT) % kAT, tz = i / (kAT * kAT);
+    const int gx = lo[0] - 1 + tx, gy = lo[1] - 1 + ty, gz = lo[2] - 1 + tz;
+    if (gx < 0 || gy < 0 || gz < 0 || gx >= rp.nx || gy >= rp.ny || gz >= rp.nz) continue;
+    atomicAdd(ob + ((int64_t)gz * rp.ny + gy) * rp.nx + gx, val);
   }
 }
 
 int adjoint_impl(Plan* p, const float* sino, int batch, float* out, cudaStream_t st) {
   const GeomParams& gp = p->gp;
   RayParams rp = make_ray_params(gp);
-  const int tiles = ((gp.nu + kTileU - 1) / kTileU) * ((gp.nv + kTileV - 1) / kTileV);
   const int64_t vox = (int64_t)gp.nx * gp.ny * gp.nz;
-  const int64_t padn = (int64_t)(gp.nx + 2 * kPad) * (gp.ny + 2 * kPad) * (gp.nz + 2 * kPad);
-  for (int b = 0; b < batch; ++b) {
-    DTV_CUDA_TRY(cudaMemsetAsync(p->d_adj_pad, 0, padn * sizeof(float), st));
-    adjoint_kernel<<<dim3(tiles, gp.n_views, 1), kFPThreads, 0, st>>>(rp, p->d_fpv, sino,
-                                                                     p->d_adj_pad, b); note_launch();
-    DTV_LAUNCH_CHECK();
-    unpad_kernel<<<grid_for(vox), 256, 0, st>>>(p->d_adj_pad, out + b * vox, gp.nx, gp.ny, gp.nz); note_launch();
-    DTV_LAUNCH_CHECK();
-  }
+  const int bricks = ((gp.nx + kAB - 1) / kAB) * ((gp.ny + kAB - 1) / kAB) *
+                     ((gp.nz + kAB - 1) / kAB);
+  DTV_CUDA_TRY(cudaMemsetAsync(out, 0, vox * batch * sizeof(float), st));
+  adjoint_brick_kernel<<<dim3(bricks, batch), kAdjThreads, 0, st>>>(rp, p->d_fpv, p->d_bpv, sino,
+                                                                    out); note_launch();
+  DTV_LAUNCH_CHECK();
   return DTV_OK;
 }
 

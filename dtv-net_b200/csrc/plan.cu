@@ -56,7 +56,6 @@ void free_plan(Plan* p) {
   cudaFree(p->d_bpv);
   cudaFree(p->d_vol_pad);
   cudaFree(p->d_sino_pad);
-  cudaFree(p->d_adj_pad);
   delete p;
 }
 
@@ -132,7 +131,6 @@ int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Pla
   const int64_t sino_pad = (int64_t)(gp.nu + 2 * kPad) * (gp.nv + 2 * kPad) * gp.n_views;
   PLAN_CUDA(cudaMalloc(&p->d_sino_pad, sizeof(float) * sino_pad));
   PLAN_CUDA(cudaMemset(p->d_sino_pad, 0, sizeof(float) * sino_pad));
-  PLAN_CUDA(cudaMalloc(&p->d_adj_pad, sizeof(float) * p->pad_elems));
 
   if (flags & DTV_PLAN_TEX) {
     p->vol_arrays = (cudaArray_t*)calloc(max_batch, sizeof(cudaArray_t));

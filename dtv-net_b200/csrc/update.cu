@@ -32,6 +32,18 @@ static inline int blocks_for(int64_t n, int threads = 256, int per_sm = 8) {
   return (int)std::max<int64_t>(1, std::min<int64_t>(b, 148LL * per_sm));
 }
 
+// Shared-memory histogram words are 32-bit; a block may add at most this many
+// elements to one (see hist_add).
+constexpr int64_t kHistBlockElems = 1LL << 20;
+
+// Grid of a histogram pass over n elements: enough blocks that none adds
+// more than kHistBlockElems elements.
+static inline int hist_blocks(int64_t n, int threads, int per_sm, int64_t per_thread) {
+  const int64_t need = (n + kHistBlockElems - 1) / kHistBlockElems;
+  return (int)std::max<int64_t>(blocks_for((n + per_thread - 1) / per_thread, threads, per_sm),
+                                need);
+}
+
 struct Dims {
   int X, Y, Z;
   int64_t N;  // X*Y*Z
@@ -217,26 +229,32 @@ __device__ __forceinline__ unsigned int sig24(unsigned int key) {
   return (key & 0x7F800000u) ? (m | 0x800000u) : m;
 }
 
-// Adds `key` to a shared histogram with warp aggregation (all lanes call;
-// lanes with active == false contribute nothing).
-__device__ __forceinline__ void hist_add(unsigned int* cnt, unsigned long long* sum, int bin,
-                                         unsigned int key, bool active) {
-  const unsigned int act = __ballot_sync(0xffffffffu, active);
+// Shared-memory histograms hold three 32-bit words per bin: the count and
+// the sums of the low and high 12 bits of each element's 24-bit significand
+// (h[0..nb) counts, h[nb..2nb) low sums, h[2nb..3nb) high sums). Each block
+// adds at most 2^20 elements, so no word overflows; hist_flush folds them
+// into the exact 64-bit sums of the global histogram.
+
+__device__ __forceinline__ void hist_add(unsigned int* h, int nb, int bin, unsigned int key,
+                                         bool active) {
   if (!active) return;
-  const unsigned int grp = __match_any_sync(act, bin);
-  const unsigned int s = __reduce_add_sync(grp, sig24(key));
-  if ((ltid() & 31) == __ffs(grp) - 1) {
-    atomicAdd(cnt + bin, (unsigned int)__popc(grp));
-    atomicAdd(sum + bin, (unsigned long long)s);
-  }
+  const unsigned int sig = sig24(key);
+  atomicAdd(h + bin, 1u);
+  atomicAdd(h + nb + bin, sig & 0xFFFu);
+  atomicAdd(h + 2 * nb + bin, sig >> 12);
 }
 
-__device__ __forceinline__ void hist_flush(const unsigned int* scnt, const unsigned long long* ssum,
-                                           unsigned int* gcnt, unsigned long long* gsum, int nb) {
+__device__ __forceinline__ void hist_clear(unsigned int* h, int nb) {
+  for (int i = ltid(); i < 3 * nb; i += lthreads()) h[i] = 0u;
+}
+
+__device__ __forceinline__ void hist_flush(const unsigned int* h, int nb, unsigned int* gcnt,
+                                           unsigned long long* gsum) {
   for (int i = ltid(); i < nb; i += lthreads()) {
-    if (scnt[i]) {
-      atomicAdd(gcnt + i, scnt[i]);
-      atomicAdd(gsum + i, ssum[i]);
+    if (h[i]) {
+      atomicAdd(gcnt + i, h[i]);
+      atomicAdd(gsum + i, (unsigned long long)h[nb + i] +
+                              ((unsigned long long)h[2 * nb + i] << 12));
     }
   }
 }
@@ -247,45 +265,45 @@ template <int C>
 __global__ void l1_hist_kernel(const float* __restrict__ x0, const float* __restrict__ x1,
                                const float* __restrict__ x2, int64_t n, L1Chan* chans, int level) {
   static_assert(C == 1, "one channel");
-  __shared__ unsigned int scnt[kL1B3];
-  __shared__ unsigned long long ssum[kL1B3];
+  __shared__ unsigned int hs[3 * kL1B3];
   L1Chan& ch = chans[0];
   if (ch.done) return;
   const int nb = level == 2 ? kL1B2 : kL1B3;
-  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
-    scnt[i] = 0;
-    ssum[i] = 0;
-  }
+  hist_clear(hs, nb);
   const unsigned int pre = ch.prefix;
   const int pshift = level == 2 ? kL1S1 : kL1S2;
   __syncthreads();
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  const int64_t nround = (n + stride - 1) / stride * stride;  // all lanes iterate together
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nround; t += stride) {
-    unsigned int key = 0;
-    bool act = false;
-    if (t < n) {
-      key = __float_as_uint(__ldg(x0 + t)) & 0x7FFFFFFFu;
-      act = (key >> pshift) == pre;
-    }
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const unsigned int key = __float_as_uint(__ldg(x0 + t)) & 0x7FFFFFFFu;
     const int bin = level == 2 ? (int)((key >> kL1S2) & (kL1B2 - 1)) : (int)(key & (kL1B3 - 1));
-    hist_add(scnt, ssum, bin, key, act);
+    hist_add(hs, nb, bin, key, (key >> pshift) == pre);
   }
   __syncthreads();
-  if (level == 2) hist_flush(scnt, ssum, ch.cnt2, ch.sum2, kL1B2);
-  else hist_flush(scnt, ssum, ch.cnt3, ch.sum3, kL1B3);
+  if (level == 2) hist_flush(hs, nb, ch.cnt2, ch.sum2);
+  else hist_flush(hs, nb, ch.cnt3, ch.sum3);
 }
 
 // Level-2 or level-3 pass over three channels at once (the fused PDHG path);
-// dynamic shared memory: 3 x bins x 12 bytes.
+// dynamic shared memory: 3 channels x 3 words x bins. Each thread loads 4
+// consecutive elements of each channel per step (16-byte loads); the arrays
+// are 16-byte aligned and the last n % 4 elements are done by block 0.
+__device__ __forceinline__ void hist3_one(unsigned int* hs, int nb, int level, const bool* live,
+                                          const unsigned int* pre, int pshift, const float (&x)[3]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const unsigned int key = __float_as_uint(x[c]) & 0x7FFFFFFFu;
+    const int bin = level == 2 ? (int)((key >> kL1S2) & (kL1B2 - 1)) : (int)(key & (kL1B3 - 1));
+    hist_add(hs + c * 3 * nb, nb, bin, key, live[c] && (key >> pshift) == pre[c]);
+  }
+}
+
 __global__ void __launch_bounds__(512) l1_hist3_kernel(const float* __restrict__ x0,
                                                        const float* __restrict__ x1,
                                                        const float* __restrict__ x2, int64_t n,
                                                        L1Chan* chans, int level) {
-  extern __shared__ unsigned char smem[];
+  extern __shared__ unsigned int hs[];
   const int nb = level == 2 ? kL1B2 : kL1B3;
-  unsigned int* scnt = reinterpret_cast<unsigned int*>(smem);
-  unsigned long long* ssum = reinterpret_cast<unsigned long long*>(smem + 3 * nb * 4);
   bool live[3];
   unsigned int pre[3];
 #pragma unroll
@@ -294,58 +312,56 @@ __global__ void __launch_bounds__(512) l1_hist3_kernel(const float* __restrict__
     pre[c] = chans[c].prefix;
   }
   if (!live[0] && !live[1] && !live[2]) return;
-  for (int i = threadIdx.x; i < 3 * nb; i += blockDim.x) {
-    scnt[i] = 0;
-    ssum[i] = 0;
-  }
+  for (int i = threadIdx.x; i < 9 * nb; i += blockDim.x) hs[i] = 0u;
   __syncthreads();
   const int pshift = level == 2 ? kL1S1 : kL1S2;
-  const float* xs[3] = {x0, x1, x2};
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  const int64_t nround = (n + stride - 1) / stride * stride;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nround; t += stride) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      unsigned int key = 0;
-      bool act = false;
-      if (t < n && live[c]) {
-        key = __float_as_uint(__ldg(xs[c] + t)) & 0x7FFFFFFFu;
-        act = (key >> pshift) == pre[c];
-      }
-      const int bin =
-          level == 2 ? (int)((key >> kL1S2) & (kL1B2 - 1)) : (int)(key & (kL1B3 - 1));
-      hist_add(scnt + c * nb, ssum + c * nb, bin, key, act);
+  const int64_t n4 = n / 4;
+  const float4* v0 = reinterpret_cast<const float4*>(x0);
+  const float4* v1 = reinterpret_cast<const float4*>(x1);
+  const float4* v2 = reinterpret_cast<const float4*>(x2);
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n4;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a, c = a;
+    if (live[0]) a = __ldg(v0 + t);
+    if (live[1]) b = __ldg(v1 + t);
+    if (live[2]) c = __ldg(v2 + t);
+    const float e0[3] = {a.x, b.x, c.x}, e1[3] = {a.y, b.y, c.y};
+    const float e2[3] = {a.z, b.z, c.z}, e3[3] = {a.w, b.w, c.w};
+    hist3_one(hs, nb, level, live, pre, pshift, e0);
+    hist3_one(hs, nb, level, live, pre, pshift, e1);
+    hist3_one(hs, nb, level, live, pre, pshift, e2);
+    hist3_one(hs, nb, level, live, pre, pshift, e3);
+  }
+  if (blockIdx.x == 0) {  // tail: the last n % 4 elements
+    const int64_t t = n4 * 4 + threadIdx.x;
+    if (t < n) {
+      const float e[3] = {live[0] ? x0[t] : 0.f, live[1] ? x1[t] : 0.f, live[2] ? x2[t] : 0.f};
+      hist3_one(hs, nb, level, live, pre, pshift, e);
     }
   }
   __syncthreads();
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     if (!live[c]) continue;
-    if (level == 2) hist_flush(scnt + c * nb, ssum + c * nb, chans[c].cnt2, chans[c].sum2, nb);
-    else hist_flush(scnt + c * nb, ssum + c * nb, chans[c].cnt3, chans[c].sum3, nb);
+    if (level == 2) hist_flush(hs + c * 3 * nb, nb, chans[c].cnt2, chans[c].sum2);
+    else hist_flush(hs + c * 3 * nb, nb, chans[c].cnt3, chans[c].sum3);
   }
 }
 
 // Level-1 histogram of a plain array (standalone L1-ball).
 __global__ void l1_hist1_kernel(const float* __restrict__ v, int64_t n, L1Chan* ch) {
-  __shared__ unsigned int scnt[kL1B1];
-  __shared__ unsigned long long ssum[kL1B1];
-  for (int i = threadIdx.x; i < kL1B1; i += blockDim.x) {
-    scnt[i] = 0;
-    ssum[i] = 0;
-  }
+  __shared__ unsigned int hs[3 * kL1B1];
+  hist_clear(hs, kL1B1);
   __syncthreads();
   unsigned int kmax = 0;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  const int64_t nround = (n + stride - 1) / stride * stride;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nround; t += stride) {
-    unsigned int key = 0;
-    if (t < n) key = __float_as_uint(__ldg(v + t)) & 0x7FFFFFFFu;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const unsigned int key = __float_as_uint(__ldg(v + t)) & 0x7FFFFFFFu;
     kmax = max(kmax, key);
-    hist_add(scnt, ssum, (int)(key >> kL1S1), key, t < n);
+    hist_add(hs, kL1B1, (int)(key >> kL1S1), key, true);
   }
   __syncthreads();
-  hist_flush(scnt, ssum, ch->cnt1, ch->sum1, kL1B1);
+  hist_flush(hs, kL1B1, ch->cnt1, ch->sum1);
   for (int o = 16; o > 0; o >>= 1) kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
   if ((threadIdx.x & 31) == 0 && kmax) atomicMax(&ch->maxkey, kmax);
 }
@@ -508,51 +524,55 @@ __global__ void __launch_bounds__(256) pdhg_dual_kernel(const T* __restrict__ fb
                                                         float* __restrict__ c, Dims d, float a0,
                                                         float a1, float a2, float smu,
                                                         L1Chan* chans) {
-  __shared__ unsigned int scnt[3][kL1B1];
-  __shared__ unsigned long long ssum[3][kL1B1];
-  for (int i = ltid(); i < 3 * kL1B1; i += lthreads()) {
-    (&scnt[0][0])[i] = 0;
-    (&ssum[0][0])[i] = 0;
-  }
+  __shared__ unsigned int hs[3][3 * kL1B1];
+  for (int i = ltid(); i < 9 * kL1B1; i += lthreads()) (&hs[0][0])[i] = 0u;
   __syncthreads();
   const Col cl = col3(d);
   unsigned int kmax[3] = {0u, 0u, 0u};
   const T* fb = fbar + cl.base;
   const int64_t plane = (int64_t)d.X * d.Y;
   const int64_t oy = axis_off(d, 1);
-  int64_t i = ((int64_t)cl.z0 * d.Y + cl.y) * d.X + cl.x;
-  float fc = cl.in ? load_as_float(fb, i) : 0.f;  // f(i), carried along z
-  for (int k = 0; k < kZS; ++k, i += plane) {
-    const bool in = cl.in && k < cl.nz;
-    unsigned int key[3] = {0u, 0u, 0u};
-    if (in) {
+  const int64_t i0 = ((int64_t)cl.z0 * d.Y + cl.y) * d.X + cl.x;
+  const bool xv = cl.x < d.X - 1;
+  const bool yv_clean = cl.y < d.Y - 1;
+  // phase 1: all slices' loads, stencils and stores (independent across k)
+  unsigned int keys[3][kZS];
+#pragma unroll
+  for (int k = 0; k < kZS; ++k) {
+    keys[0][k] = keys[1][k] = keys[2][k] = 0u;
+    if (cl.in && k < cl.nz) {
+      const int64_t i = i0 + k * plane;
       const int z = cl.z0 + k;
-      const float fz = z < d.Z - 1 ? load_as_float(fb, i + plane) : 0.f;
-      const float gx = cl.x < d.X - 1 ? load_as_float(fb, i + 1) - fc : -fc;
-      const bool yv = d.quirk ? (i < d.N - d.Y) : (cl.y < d.Y - 1);
+      const float fc = load_as_float(fb, i);
+      const float gx = xv ? load_as_float(fb, i + 1) - fc : -fc;
+      const bool yv = d.quirk ? (i < d.N - d.Y) : yv_clean;
       const float gy = yv ? load_as_float(fb, i + oy) - fc : -fc;
-      const float gz = z < d.Z - 1 ? fz - fc : -fc;
+      const float gz = z < d.Z - 1 ? load_as_float(fb, i + plane) - fc : -fc;
       const int64_t t = cl.base + i;
       const float np = fmaf(a0, gx, p[t]), nq = fmaf(a1, gy, q[t]), ns = fmaf(a2, gz, s[t]);
       p[t] = np;
       q[t] = nq;
       s[t] = ns;
       c[t] = fminf(fmaf(smu, fc, c[t]), 0.f);  // -relu(-c - sigma*mu*fbar)
-      key[0] = __float_as_uint(np) & 0x7FFFFFFFu;
-      key[1] = __float_as_uint(nq) & 0x7FFFFFFFu;
-      key[2] = __float_as_uint(ns) & 0x7FFFFFFFu;
-      kmax[0] = max(kmax[0], key[0]);
-      kmax[1] = max(kmax[1], key[1]);
-      kmax[2] = max(kmax[2], key[2]);
-      fc = fz;
+      keys[0][k] = __float_as_uint(np) & 0x7FFFFFFFu;
+      keys[1][k] = __float_as_uint(nq) & 0x7FFFFFFFu;
+      keys[2][k] = __float_as_uint(ns) & 0x7FFFFFFFu;
     }
+  }
+  // phase 2: level-1 histograms (warp-synchronous; every lane takes part)
 #pragma unroll
-    for (int a = 0; a < 3; ++a) hist_add(scnt[a], ssum[a], (int)(key[a] >> kL1S1), key[a], in);
+  for (int k = 0; k < kZS; ++k) {
+    const bool in = cl.in && k < cl.nz;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      kmax[a] = max(kmax[a], keys[a][k]);
+      hist_add(hs[a], kL1B1, (int)(keys[a][k] >> kL1S1), keys[a][k], in);
+    }
   }
   __syncthreads();
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    hist_flush(scnt[a], ssum[a], chans[a].cnt1, chans[a].sum1, kL1B1);
+    hist_flush(hs[a], kL1B1, chans[a].cnt1, chans[a].sum1);
     unsigned int km = kmax[a];
     for (int o = 16; o > 0; o >>= 1) km = max(km, __shfl_xor_sync(0xffffffffu, km, o));
     if ((ltid() & 31) == 0 && km) atomicMax(&chans[a].maxkey, km);
@@ -789,11 +809,11 @@ int dtv_l1ball(const float* v, float* w, int64_t n, const double* radius, void* 
   cudaStream_t st = as_stream(stream);
   L1Chan* ch = reinterpret_cast<L1Chan*>(ws);
   l1_reset_kernel<<<1, 32, 0, st>>>(ch, 1, radius, nullptr, 0.f, 0.f, 0.f); note_launch();
-  l1_hist1_kernel<<<blocks_for(n, 256, 4), 256, 0, st>>>(v, n, ch); note_launch();
+  l1_hist1_kernel<<<hist_blocks(n, 256, 4, 1), 256, 0, st>>>(v, n, ch); note_launch();
   l1_select_kernel<<<1, 1024, 0, st>>>(ch, 1); note_launch();
-  l1_hist_kernel<1><<<blocks_for(n, 256, 4), 256, 0, st>>>(v, nullptr, nullptr, n, ch, 2); note_launch();
+  l1_hist_kernel<1><<<hist_blocks(n, 256, 4, 1), 256, 0, st>>>(v, nullptr, nullptr, n, ch, 2); note_launch();
   l1_select_kernel<<<1, 1024, 0, st>>>(ch, 2); note_launch();
-  l1_hist_kernel<1><<<blocks_for(n, 256, 4), 256, 0, st>>>(v, nullptr, nullptr, n, ch, 3); note_launch();
+  l1_hist_kernel<1><<<hist_blocks(n, 256, 4, 1), 256, 0, st>>>(v, nullptr, nullptr, n, ch, 3); note_launch();
   l1_select_kernel<<<1, 1024, 0, st>>>(ch, 3); note_launch();
   l1_apply_kernel<<<blocks_for(n), 256, 0, st>>>(v, w, n, ch, lambda_out); note_launch();
   DTV_LAUNCH_CHECK();
@@ -830,17 +850,18 @@ int dtv_pdhg_dual(const void* fbar, float* p, float* q, float* s, float* c, cons
   }
   DTV_LAUNCH_CHECK();
   static bool attr = false;
-  const int smem3 = 3 * kL1B3 * (int)(sizeof(unsigned int) + sizeof(unsigned long long));
+  const int smem3 = 9 * kL1B3 * (int)sizeof(unsigned int);
   if (!attr) {
     DTV_CUDA_TRY(cudaFuncSetAttribute(l1_hist3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       smem3));
     attr = true;
   }
-  const int smem2 = 3 * kL1B2 * (int)(sizeof(unsigned int) + sizeof(unsigned long long));
+  const int smem2 = 9 * kL1B2 * (int)sizeof(unsigned int);
   l1_select_kernel<<<3, 1024, 0, st>>>(ch, 1); note_launch();
-  l1_hist3_kernel<<<blocks_for(total, 512, 2), 512, smem2, st>>>(p, q, s, total, ch, 2); note_launch();
+  DTV_CHECK(((uintptr_t)p | (uintptr_t)q | (uintptr_t)s) % 16 == 0, "p, q, s must be 16-byte aligned");
+  l1_hist3_kernel<<<hist_blocks(total, 512, 2, 4), 512, smem2, st>>>(p, q, s, total, ch, 2); note_launch();
   l1_select_kernel<<<3, 1024, 0, st>>>(ch, 2); note_launch();
-  l1_hist3_kernel<<<blocks_for(total, 512, 2), 512, smem3, st>>>(p, q, s, total, ch, 3); note_launch();
+  l1_hist3_kernel<<<hist_blocks(total, 512, 2, 4), 512, smem3, st>>>(p, q, s, total, ch, 3); note_launch();
   l1_select_kernel<<<3, 1024, 0, st>>>(ch, 3); note_launch();
   DTV_LAUNCH_CHECK();
   return DTV_OK;
@@ -999,11 +1020,11 @@ extern "C" int dtv_l1ball_noalloc(const float* v, float* w, int64_t n, const dou
   // start at zero, so clear the whole workspace first.
   DTV_CUDA_TRY(cudaMemsetAsync(ch, 0, sizeof(L1Chan), st));
   l1_reset_kernel<<<1, 32, 0, st>>>(ch, 1, radius, nullptr, 0.f, 0.f, 0.f); note_launch();
-  l1_hist1_kernel<<<blocks_for(n, 256, 4), 256, 0, st>>>(v, n, ch); note_launch();
+  l1_hist1_kernel<<<hist_blocks(n, 256, 4, 1), 256, 0, st>>>(v, n, ch); note_launch();
   l1_select_kernel<<<1, 1024, 0, st>>>(ch, 1); note_launch();
-  l1_hist_kernel<1><<<blocks_for(n, 256, 4), 256, 0, st>>>(v, nullptr, nullptr, n, ch, 2); note_launch();
+  l1_hist_kernel<1><<<hist_blocks(n, 256, 4, 1), 256, 0, st>>>(v, nullptr, nullptr, n, ch, 2); note_launch();
   l1_select_kernel<<<1, 1024, 0, st>>>(ch, 2); note_launch();
-  l1_hist_kernel<1><<<blocks_for(n, 256, 4), 256, 0, st>>>(v, nullptr, nullptr, n, ch, 3); note_launch();
+  l1_hist_kernel<1><<<hist_blocks(n, 256, 4, 1), 256, 0, st>>>(v, nullptr, nullptr, n, ch, 3); note_launch();
   l1_select_kernel<<<1, 1024, 0, st>>>(ch, 3); note_launch();
   l1_apply_kernel<<<blocks_for(n), 256, 0, st>>>(v, w, n, ch, lambda_out); note_launch();
   DTV_LAUNCH_CHECK();
