@@ -415,6 +415,126 @@ def run_ours(args):
     return 0
 
 
+def run_batch16(args):
+    """16 heterogeneous reconstructions: edges seeded uniform in {96,128,192,256},
+    30-120 views, square detector 1.5x the edge (pitch 1.5 mm, voxel 1 mm),
+    30 FISTA iterations each. Batched = one graph with a stream per
+    reconstruction; plain = the same reconstructions one after another, eager."""
+    import numpy as np
+    import torch
+
+    import dtvb200
+    from dtvb200.phantom import ellipsoids
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(16)
+    algs, plains, imgs, sinos, units = [], [], [], [], 0.0
+    specs = []
+    for i in range(16):
+        n = int(rng.choice([96, 128, 192, 256]))
+        views = int(rng.integers(30, 121))
+        d = int(round(1.5 * n))
+        ang = np.linspace(0, 360, views, endpoint=False)
+        geo = dtvb200.circular(ang, (n, n, n), (1.0,) * 3, (d, d), (1.5, 1.5), 500.0, 1000.0)
+        plan = dtvb200.Plan(geo, sampler=args.sampler, device=dev)
+        truth = ellipsoids((n, n, n), seed=100 + i, device=dev)
+        sino = plan.forward(truth)
+        algs.append(dtvb200.FISTA(plan, 30, lamb=0.05, L=1e-3))
+        plains.append(dtvb200.FISTA(plan, 30, lamb=0.05, L=1e-3))
+        imgs.append(torch.zeros_like(truth))
+        sinos.append(sino)
+        units += 30 * (plan.fp_samples() + n ** 3 * views)
+        specs.append((n, views))
+    batch = dtvb200.Batched(algs, use_graph=True)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(max(args.warmup, 1)):
+        batch.run(imgs, sinos)
+    with ClockSampler(0) as clk:
+        secs = time_steps(lambda: batch.run(imgs, sinos), args.steps, stream)
+
+    def plain_all():
+        for a, i, s in zip(plains, imgs, sinos):
+            a.run(i, s)
+
+    plain_all()
+    ps = time_steps(plain_all, args.steps, stream)
+    line = {
+        "metric": METRIC, "value": units * args.steps / secs / 1e9, "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "16 heterogeneous FISTA reconstructions (30 iterations each), "
+                               "edges in {96,128,192,256}, 30-120 views, detector 1.5x edge",
+                   "sizes_views": specs, "sampler": args.sampler},
+        "recon_per_s": 16 * args.steps / secs,
+        "plain_sequential_eager": {"value": units * args.steps / ps / 1e9,
+                                   "recon_per_s": 16 * args.steps / ps},
+        "gpu_launches": batch.launches_per_run * args.steps,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_train(args):
+    """Training steps of a 10-stage unrolled PDHG network (learned steps + a
+    3-layer 3x3x3 conv block with 32 channels per stage, BF16 activations,
+    FP32 weights, per-stage checkpointing) on a batch of two 128^3 phantoms
+    seen by 48 views of 192x192 (pitch 1.5 mm): L2 loss, Adam. The data
+    steps and their gradients go through the matched projector pair."""
+    import numpy as np
+    import torch
+
+    import dtvb200
+    from dtvb200.nets import UnrolledPDHG
+    from dtvb200.phantom import ellipsoids
+    dev = torch.device("cuda", 0)
+    n, views, det, stages = 128, 48, 192, 10
+    ang = np.linspace(0, 360, views, endpoint=False)
+    geo = dtvb200.circular(ang, (n, n, n), (1.0,) * 3, (det, det), (1.5, 1.5), 500.0, 1000.0)
+    proj = dtvb200.Projector(geo, max_batch=2)
+    truth = torch.cat([ellipsoids((n, n, n), seed=s, device=dev) for s in (1, 2)])
+    sino = proj.fp_soft(truth)
+    torch.manual_seed(0)
+    net = UnrolledPDHG(proj, stages=stages, features=32, lamb=1e-3, tau=1e-3).to(dev)
+    opt = torch.optim.Adam(net.parameters(), lr=1e-4)
+    x0 = torch.zeros_like(truth)
+
+    def step():
+        opt.zero_grad(set_to_none=True)
+        loss = torch.mean((net(x0, sino) - truth) ** 2)
+        loss.backward()
+        opt.step()
+        return loss
+
+    for _ in range(max(args.warmup, 1)):
+        step()
+    stream = torch.cuda.current_stream(dev)
+    L = dtvb200._lib.load()
+    n0 = L.dtv_launch_count()
+    with ClockSampler(0) as clk:
+        secs = time_steps(step, args.steps, stream)
+    launches = L.dtv_launch_count() - n0
+    plan = proj.plan(dev, 2)
+    fp_units = 2 * plan.fp_samples()  # per forward projection of the batch
+    # per training step: each stage runs FP + A^T forward, recomputes them under
+    # checkpointing, and backpropagates through both (FP + A^T again)
+    units = stages * 3 * 2 * fp_units
+    line = {
+        "metric": "unrolled-net training steps/s (projector pair through the exact adjoint)",
+        "value": args.steps / secs, "unit": "steps/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 projectors, bf16 conv activations",
+        "data": "synthetic",
+        "config": {"workload": "10-stage unrolled PDHG net, batch 2 x 128^3, 48 views of 192^2",
+                   "checkpointing": "per stage"},
+        "projector_gsamples_per_s": units * args.steps / secs / 1e9,
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_profile(args):
     """N eager iterations of the workload (for ncu): forward projector,
     backprojector and fused updates, one launch each per iteration."""
@@ -449,6 +569,11 @@ def main():
     ap.add_argument("--small", action="store_true", help="64^3 smoke-size workload")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", choices=["sparse_dtv", "batch16", "train"],
+                    default="sparse_dtv",
+                    help="sparse_dtv: the headline workload; batch16: 16 heterogeneous FISTA "
+                         "reconstructions batched into one graph; train: training steps of a "
+                         "10-stage unrolled network through the exact adjoint")
     ap.add_argument("--profile", type=int, default=0, metavar="N",
                     help="profiling run: N eager DTV iterations of the workload, no timing")
     args = ap.parse_args()
@@ -458,6 +583,10 @@ def main():
         return run_reference(args)
     if args.profile:
         return run_profile(args)
+    if args.workload == "batch16":
+        return run_batch16(args)
+    if args.workload == "train":
+        return run_train(args)
     return run_ours(args)
 
 

@@ -127,6 +127,8 @@ struct Plan {
   cudaTextureObject_t* pair_tex;
   cudaSurfaceObject_t* pair_surf;
   cudaTextureObject_t* pair_tex_dev;
+  // adjoint ray table (DTV_PLAN_ADJOINT): per view and pixel, (p0, count) and (dp, 0)
+  float4* d_rays;
   double fp_samples;  // per volume, < 0 until computed
 };
 
@@ -138,5 +140,6 @@ int forward_impl(Plan* p, const void* vol, int vol_dtype, int batch, float* out,
 int backward_impl(Plan* p, const float* sino, int batch, float* out, int accumulate,
                   cudaStream_t st);
 int adjoint_impl(Plan* p, const float* sino, int batch, float* out, cudaStream_t st);
+int build_ray_table(Plan* p, cudaStream_t st);
 
 }  // namespace dtv

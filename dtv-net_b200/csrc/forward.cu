@@ -480,13 +480,39 @@ int forward_impl(Plan* p, const void* vol, int vol_dtype, int batch, float* out,
 // brick (the first brick along an axis also takes base -1, whose upper taps
 // are inside). Every contributing sample belongs to exactly one brick, so the
 // sum is the exact transpose; each brick then adds its tile to the output once.
+// Ray table: rays[2*r] = (p0, count), rays[2*r+1] = (dp, 0) for ray r = (n*nv + v)*nu + u.
+__global__ void ray_table_kernel(RayParams rp, const FPView* __restrict__ views,
+                                 float4* __restrict__ rays) {
+  const int64_t total = (int64_t)rp.n_views * rp.nu * rp.nv;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < total;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const int u = (int)(r % rp.nu);
+    const int64_t q = r / rp.nu;
+    const int v = (int)(q % rp.nv), n = (int)(q / rp.nv);
+    const RaySetup rs = setup_ray(rp, views[n], u, v);
+    const int c = rs.count > 0 ? rs.count : 0;
+    rays[2 * r] = make_float4(c ? rs.p0[0] : 0.f, c ? rs.p0[1] : 0.f, c ? rs.p0[2] : 0.f,
+                              __int_as_float(c));
+    rays[2 * r + 1] = make_float4(c ? rs.dp[0] : 0.f, c ? rs.dp[1] : 0.f, c ? rs.dp[2] : 0.f, 0.f);
+  }
+}
+
+int build_ray_table(Plan* p, cudaStream_t st) {
+  RayParams rp = make_ray_params(p->gp);
+  const int64_t total = (int64_t)rp.n_views * rp.nu * rp.nv;
+  ray_table_kernel<<<grid_for(total), 256, 0, st>>>(rp, p->d_fpv, p->d_rays); note_launch();
+  DTV_LAUNCH_CHECK();
+  return DTV_OK;
+}
+
 constexpr int kAB = 16;         // brick edge (voxels)
 constexpr int kAT = kAB + 2;    // tile edge: voxels lo-1 .. lo+kAB
 constexpr int kAdjThreads = 256;
 
+template <bool kTable>
 __global__ void __launch_bounds__(kAdjThreads) adjoint_brick_kernel(
     RayParams rp, const FPView* __restrict__ views, const BPView* __restrict__ pviews,
-    const float* __restrict__ sino, float* __restrict__ out) {
+    const float4* __restrict__ rays, const float* __restrict__ sino, float* __restrict__ out) {
   __shared__ float tile[kAT * kAT * kAT];
   const int nbx = (rp.nx + kAB - 1) / kAB, nby = (rp.ny + kAB - 1) / kAB;
   const int bid = blockIdx.x;
@@ -526,13 +552,21 @@ __global__ void __launch_bounds__(kAdjThreads) adjoint_brick_kernel(
     if (u0 > u1 || v0 > v1) continue;
     const int w = u1 - u0 + 1;
     const int cnt = w * (v1 - v0 + 1);
-    const FPView& f = views[n];
     const float* sv = sb + n * per_view;
-    for (int r = threadIdx.x; r < cnt; r += blockDim.x) {
+    for (int r = threadIdx.x; r < cnt; r += blockDim.x) {  // one ray per thread
       const int u = u0 + r % w, v = v0 + r / w;
       const float y = __ldg(sv + (int64_t)v * rp.nu + u) * rp.scale;
       if (y == 0.f) continue;
-      const RaySetup rs = setup_ray(rp, f, u, v);
+      RaySetup rs;
+      if constexpr (kTable) {
+        const int64_t r2 = 2 * (((int64_t)n * rp.nv + v) * rp.nu + u);
+        const float4 a = __ldg(rays + r2), d = __ldg(rays + r2 + 1);
+        rs.p0[0] = a.x; rs.p0[1] = a.y; rs.p0[2] = a.z;
+        rs.count = __float_as_int(a.w);
+        rs.dp[0] = d.x; rs.dp[1] = d.y; rs.dp[2] = d.z;
+      } else {
+        rs = setup_ray(rp, views[n], u, v);
+      }
       if (rs.count <= 0) continue;
       // samples that can have their base in this brick (one-sample margin)
       float kl = 0.f, kh = (float)rs.count;
@@ -548,7 +582,7 @@ __global__ void __launch_bounds__(kAdjThreads) adjoint_brick_kernel(
           miss = true;
         }
       }
-      if (miss) continue;
+      if (miss || !(kh >= kl)) continue;
       const int k0 = max(0, (int)floorf(kl) - 1);
       const int k1 = min(rs.count, (int)ceilf(kh) + 1);
       for (int k = k0; k < k1; ++k) {
@@ -594,8 +628,13 @@ int adjoint_impl(Plan* p, const float* sino, int batch, float* out, cudaStream_t
   const int bricks = ((gp.nx + kAB - 1) / kAB) * ((gp.ny + kAB - 1) / kAB) *
                      ((gp.nz + kAB - 1) / kAB);
   DTV_CUDA_TRY(cudaMemsetAsync(out, 0, vox * batch * sizeof(float), st));
-  adjoint_brick_kernel<<<dim3(bricks, batch), kAdjThreads, 0, st>>>(rp, p->d_fpv, p->d_bpv, sino,
-                                                                    out); note_launch();
+  if (p->d_rays) {
+    adjoint_brick_kernel<true><<<dim3(bricks, batch), kAdjThreads, 0, st>>>(
+        rp, p->d_fpv, p->d_bpv, p->d_rays, sino, out); note_launch();
+  } else {
+    adjoint_brick_kernel<false><<<dim3(bricks, batch), kAdjThreads, 0, st>>>(
+        rp, p->d_fpv, p->d_bpv, nullptr, sino, out); note_launch();
+  }
   DTV_LAUNCH_CHECK();
   return DTV_OK;
 }

@@ -52,6 +52,7 @@ void free_plan(Plan* p) {
   free(p->sino_tex);
   free(p->sino_arrays);
   cudaFree(p->vol_tex_dev);
+  cudaFree(p->d_rays);
   cudaFree(p->d_fpv);
   cudaFree(p->d_bpv);
   cudaFree(p->d_vol_pad);
@@ -79,7 +80,8 @@ int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Pla
   DTV_CHECK(out != nullptr, "out is NULL");
   *out = nullptr;
   DTV_CHECK(max_batch > 0, "max_batch must be positive");
-  DTV_CHECK((flags & ~(DTV_PLAN_TEX | DTV_PLAN_STAGE_F16 | DTV_PLAN_TEX_PAIRS)) == 0,
+  DTV_CHECK((flags & ~(DTV_PLAN_TEX | DTV_PLAN_STAGE_F16 | DTV_PLAN_TEX_PAIRS | DTV_PLAN_ADJOINT)) ==
+                0,
             "unknown plan flags 0x%x", flags);
   DTV_CHECK(!((flags & DTV_PLAN_TEX) && (flags & DTV_PLAN_TEX_PAIRS)),
             "DTV_PLAN_TEX and DTV_PLAN_TEX_PAIRS are exclusive");
@@ -209,6 +211,19 @@ int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Pla
     PLAN_CUDA(cudaMalloc3DArray(&p->sino_arrays[0], &sd, make_cudaExtent(gp.nu, gp.nv, gp.n_views),
                                 cudaArrayLayered));
     rc = make_tex3d(p->sino_arrays[0], 1, &p->sino_tex[0]);
+    if (rc) {
+      free_plan(p);
+      return rc;
+    }
+  }
+  if (flags & DTV_PLAN_ADJOINT) {
+    const size_t n = (size_t)gp.n_views * gp.nu * gp.nv * 2;
+    PLAN_CUDA(cudaMalloc(&p->d_rays, n * sizeof(float4)));
+    rc = build_ray_table(p, 0);
+    if (!rc) {
+      cudaError_t e = cudaStreamSynchronize(0);
+      if (e != cudaSuccess) rc = fail(DTV_ERR_CUDA, "ray table: %s", cudaGetErrorString(e));
+    }
     if (rc) {
       free_plan(p);
       return rc;

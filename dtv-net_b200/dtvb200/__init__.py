@@ -9,12 +9,12 @@ from .geometry import Geometry, Plan, circular, standard, vector
 from .ops import (BeijingGeometry, Projector, StandardGeometry, StandardGeometryWithFBP,
                   make_functions)
 from .tv import diff, diff_abs_sums, l1ball
-from .algorithms import ASDPOCS, DTVCP, DTVFISTA, FISTA, power_norm
+from .algorithms import ASDPOCS, DTVCP, DTVFISTA, FISTA, Batched, power_norm
 
 __all__ = [
     "DtvError", "Geometry", "Plan", "circular", "standard", "vector", "Projector",
     "StandardGeometry", "StandardGeometryWithFBP", "BeijingGeometry", "make_functions", "diff",
-    "diff_abs_sums", "l1ball", "DTVCP", "FISTA", "DTVFISTA", "ASDPOCS", "power_norm",
+    "diff_abs_sums", "l1ball", "DTVCP", "FISTA", "DTVFISTA", "ASDPOCS", "Batched", "power_norm",
     "library_path",
 ]
 

@@ -15,6 +15,7 @@ DTV_OK, DTV_ERR_INVALID, DTV_ERR_CUDA, DTV_ERR_ALLOC, DTV_ERR_UNSUPPORTED = 0, 1
 DTV_F32, DTV_F16, DTV_BF16 = 0, 1, 2
 DTV_PHASE_STANDARD, DTV_PHASE_VECTOR, DTV_PHASE_BOX = 0, 1, 2
 DTV_PLAN_SOFT, DTV_PLAN_TEX, DTV_PLAN_STAGE_F16, DTV_PLAN_TEX_PAIRS = 0x0, 0x1, 0x2, 0x4
+DTV_PLAN_ADJOINT = 0x8
 DTV_EPI_STORE, DTV_EPI_RESIDUAL, DTV_EPI_PDHG = 0, 1, 2
 
 

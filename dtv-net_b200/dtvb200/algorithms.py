@@ -46,31 +46,81 @@ def power_norm(size, axis: int, quirk: bool = True, iters: int = 10, seed: int =
     return s
 
 
+def _run_graph(owner, key, body):
+    """Run `body` (which only enqueues work on the current stream) eagerly, or
+    capture it once per `key` as a CUDA graph on `owner` and replay it. The
+    number of this library's kernel launches per run is kept in
+    owner.launches_per_run."""
+    L = _lib.load()
+    if not owner.use_graph:
+        n0 = L.dtv_launch_count()
+        body()
+        owner.launches_per_run = L.dtv_launch_count() - n0
+        return
+    cache = owner.__dict__.setdefault("_graphs", {})
+    g = cache.get(key)
+    if g is None:
+        body()  # warm-up run (sets kernel attributes, loads modules)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        n0 = L.dtv_launch_count()
+        with torch.cuda.graph(g):
+            body()
+        owner.launches_per_run = L.dtv_launch_count() - n0
+        cache[key] = g
+    g.replay()
+
+
 class _Graphable:
-    """Runs `_iterate` eagerly or as one captured CUDA graph per input shape."""
+    """A reconstruction run as prepare (inputs into persistent buffers) ->
+    enqueue (every iteration, stream-ordered, no host sync) -> result; the
+    enqueue step runs eagerly or as one captured CUDA graph per input shape."""
 
     use_graph: bool = False
     launches_per_run: int = 0  # kernels of this library one run launches
 
     def _graph_run(self, key, body):
-        L = _lib.load()
-        if not self.use_graph:
-            n0 = L.dtv_launch_count()
-            body()
-            self.launches_per_run = L.dtv_launch_count() - n0
-            return
-        cache = self.__dict__.setdefault("_graphs", {})
-        g = cache.get(key)
-        if g is None:
-            body()  # warm-up run (sets kernel attributes, loads modules)
-            torch.cuda.synchronize()
-            g = torch.cuda.CUDAGraph()
-            n0 = L.dtv_launch_count()
-            with torch.cuda.graph(g):
-                body()
-            self.launches_per_run = L.dtv_launch_count() - n0
-            cache[key] = g
-        g.replay()
+        _run_graph(self, key, body)
+
+    def run(self, image: torch.Tensor, sino: torch.Tensor, out: torch.Tensor = None):
+        """Reconstruct from `sino` (device or host tensor) starting at `image`.
+        Returns the reconstruction as float32 (a copy in `out` if given)."""
+        key, st = self._prepare(image, sino)
+        self._graph_run(key, lambda: self._enqueue(st))
+        return self._result(st, out)
+
+
+class Batched:
+    """Several reconstructions (each with its own plan, geometry and size) run
+    as one unit: each one's iterations go on a stream of its own, so their
+    kernels overlap on the GPU, and with ``use_graph`` the whole set is one
+    captured CUDA graph (one launch per run)."""
+
+    def __init__(self, algs, use_graph: bool = True):
+        self.algs = list(algs)
+        self.use_graph = use_graph
+        self.launches_per_run = 0
+        self._streams = None
+
+    def run(self, images, sinos, outs=None):
+        if self._streams is None:
+            dev = images[0].device
+            self._streams = [torch.cuda.Stream(device=dev) for _ in self.algs]
+        prepared = [a._prepare(i, s) for a, i, s in zip(self.algs, images, sinos)]
+        key = tuple(k for k, _ in prepared)
+
+        def enqueue_all():
+            main = torch.cuda.current_stream()
+            for a, (_, st), sm in zip(self.algs, prepared, self._streams):
+                sm.wait_stream(main)
+                with torch.cuda.stream(sm):
+                    a._enqueue(st)
+            for sm in self._streams:
+                main.wait_stream(sm)
+
+        _run_graph(self, key, enqueue_all)
+        outs = outs or [None] * len(self.algs)
+        return [a._result(st, o) for a, (_, st), o in zip(self.algs, prepared, outs)]
 
 
 class DTVCP(_Graphable):
@@ -177,10 +227,7 @@ class DTVCP(_Graphable):
                  _ptr(st["q"]), _ptr(st["s"]), _ptr(st["c"]), size, b, ctypes.byref(prm),
                  _ptr(st["ws"]), stream)
 
-    def run(self, image: torch.Tensor, sino: torch.Tensor, out: torch.Tensor = None):
-        """Reconstruct from `sino` starting at `image` (DTVCP.run). Returns f
-        (float32; a copy in `out` if given). Per-iteration sum|A fbar - g| is
-        left in self.losses (device float64)."""
+    def _prepare(self, image, sino):
         check_input(image, "image", self.plan.vol_shape(image.shape[0]),
                     dtypes=(torch.float32, torch.float16))
         key = (tuple(image.shape), image.device.index)
@@ -191,7 +238,13 @@ class DTVCP(_Graphable):
             st["img"] = torch.empty_like(image, dtype=torch.float32)
         st["img"].copy_(image)
         st["g"].copy_(sino)
-        self._graph_run(key, lambda: self._body(st, st["img"]))
+        return key, st
+
+    def _enqueue(self, st):
+        self._body(st, st["img"])
+
+    def _result(self, st, out):
+        """f (float32); per-iteration sum|A fbar - g| stays in self.losses."""
         self.losses = st["loss"]
         if out is None:
             return st["f"].float().clone()
@@ -230,7 +283,7 @@ class FISTA(_Graphable):
                  self.lamb * self.L, (t - 1) / tp, stream)
             t = tp
 
-    def run(self, image: torch.Tensor, sino: torch.Tensor, out: torch.Tensor = None):
+    def _prepare(self, image, sino):
         check_input(image, "image", self.plan.vol_shape(image.shape[0]))
         key = (tuple(image.shape), image.device.index)
         st = self.__dict__.setdefault("_state", {}).get(key)
@@ -243,7 +296,12 @@ class FISTA(_Graphable):
             self._state[key] = st
         st["img"].copy_(image)
         st["g"].copy_(sino)
-        self._graph_run(key, lambda: self._body(st))
+        return key, st
+
+    def _enqueue(self, st):
+        self._body(st)
+
+    def _result(self, st, out):
         if out is None:
             return st["xp"].clone()
         out.copy_(st["xp"])
@@ -296,7 +354,7 @@ class DTVFISTA(_Graphable):
             if not self.quirk:
                 t = tp
 
-    def run(self, image: torch.Tensor, sino: torch.Tensor, out: torch.Tensor = None):
+    def _prepare(self, image, sino):
         check_input(image, "image", self.plan.vol_shape(image.shape[0]))
         key = (tuple(image.shape), image.device.index)
         st = self.__dict__.setdefault("_state", {}).get(key)
@@ -311,7 +369,12 @@ class DTVFISTA(_Graphable):
             self._state[key] = st
         st["img"].copy_(image)
         st["g"].copy_(sino)
-        self._graph_run(key, lambda: self._body(st))
+        return key, st
+
+    def _enqueue(self, st):
+        self._body(st)
+
+    def _result(self, st, out):
         if out is None:
             return st["f"].clone()
         out.copy_(st["f"])
@@ -361,7 +424,7 @@ class ASDPOCS(_Graphable):
             beta *= self.beta_red
         st["result"] = f
 
-    def run(self, image: torch.Tensor, sino: torch.Tensor, out: torch.Tensor = None):
+    def _prepare(self, image, sino):
         check_input(image, "image", self.plan.vol_shape(image.shape[0]))
         key = (tuple(image.shape), image.device.index)
         st = self.__dict__.setdefault("_state", {}).get(key)
@@ -377,7 +440,12 @@ class ASDPOCS(_Graphable):
             self._state[key] = st
         st["img"].copy_(image)
         st["g"].copy_(sino)
-        self._graph_run(key, lambda: self._body(st))
+        return key, st
+
+    def _enqueue(self, st):
+        self._body(st)
+
+    def _result(self, st, out):
         res = torch.relu(st["result"])  # (:47)
         if out is None:
             return res

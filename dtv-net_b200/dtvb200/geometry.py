@@ -137,10 +137,12 @@ class Plan:
     the reference) or "pairs" (FP16 z-plane pairs in a layered texture: one
     bilinear fetch per sample, z interpolated in FP32). The backprojector
     samples the sinogram through a texture for "tex" and "pairs".
-    ``stage_f16`` stages projected volumes as FP16 ("soft"/"tex")."""
+    ``stage_f16`` stages projected volumes as FP16 ("soft"/"tex").
+    ``adjoint`` keeps a per-ray table that speeds up :meth:`adjoint`
+    (32 bytes per ray and view)."""
 
     def __init__(self, geometry: Geometry, max_batch: int = 1, sampler: str = "soft",
-                 stage_f16: bool = False, device=None):
+                 stage_f16: bool = False, device=None, adjoint: bool = False):
         if sampler not in ("soft", "tex", "pairs"):
             raise ValueError("sampler must be 'soft', 'tex' or 'pairs'")
         dev = torch.device("cuda", torch.cuda.current_device()) if device is None else \
@@ -154,7 +156,7 @@ class Plan:
         self.sampler = sampler
         self.stage_f16 = bool(stage_f16)
         flags = {"soft": 0, "tex": _lib.DTV_PLAN_TEX, "pairs": _lib.DTV_PLAN_TEX_PAIRS}[sampler] | \
-            (_lib.DTV_PLAN_STAGE_F16 if stage_f16 else 0)
+            (_lib.DTV_PLAN_STAGE_F16 if stage_f16 else 0) | (_lib.DTV_PLAN_ADJOINT if adjoint else 0)
         h = ctypes.c_void_p()
         call("dtv_plan_create", ctypes.byref(geometry.struct), self.max_batch, flags,
              self.device.index, ctypes.byref(h))

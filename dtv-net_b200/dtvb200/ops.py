@@ -39,7 +39,8 @@ class Projector:
         if p is None or p.max_batch < batch:
             if p is not None:
                 p.close()
-            p = Plan(self.geometry, max(batch, self.max_batch), sampler, self.stage_f16, device)
+            p = Plan(self.geometry, max(batch, self.max_batch), sampler, self.stage_f16, device,
+                     adjoint=(sampler == "soft"))
             self._plans[key] = p
         return p
 

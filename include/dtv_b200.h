@@ -69,6 +69,10 @@ extern "C" {
  * returns both planes and the z interpolation is done in FP32. Backprojector
  * as DTV_PLAN_TEX. Needs nz + 3 <= the device's layered-texture layer limit. */
 #define DTV_PLAN_TEX_PAIRS 0x4
+/* Keep a table of every ray's sample range (32 bytes per ray and view) for
+ * dtv_backward_adjoint, which otherwise rebuilds each ray for every 16^3
+ * brick it crosses. */
+#define DTV_PLAN_ADJOINT 0x8
 
 /* ---- forward-projector epilogues ---------------------------------------- */
 #define DTV_EPI_STORE 0    /* out = FP(vol)                                        */

@@ -115,9 +115,10 @@ def test_backward_accumulate(cuda):
 
 
 @pytest.mark.parametrize("kind", KINDS)
-def test_adjoint_matches_oracle_and_dot_test(cuda, kind):
+@pytest.mark.parametrize("table", [False, True])
+def test_adjoint_matches_oracle_and_dot_test(cuda, kind, table):
     g, og = make_case(kind)
-    plan = dtvb200.Plan(g, max_batch=2, device=cuda)
+    plan = dtvb200.Plan(g, max_batch=2, device=cuda, adjoint=table)
     rng = np.random.default_rng(14)
     y = rng.random((2, 1) + og.sino_shape).astype(np.float32)
     x = rng.random((2, 1) + og.vol_shape).astype(np.float32)
