@@ -44,7 +44,11 @@ struct SoftBil {
   }
 };
 
-template <bool kTex>
+// kZAff: every view's u and h are independent of z (a detector parallel to the
+// rotation axis, as in the circular orbits), so per column and view the kernel
+// computes u, 1/h and the weight once and each voxel costs one FMA for v, one
+// fetch and one FMA.
+template <bool kTex, bool kZAff>
 __global__ void __launch_bounds__(kBPThreads) bp_kernel(BPParams bp, const BPView* __restrict__ views,
                                                         const float* __restrict__ spad,
                                                         cudaTextureObject_t tex,
@@ -70,24 +74,44 @@ __global__ void __launch_bounds__(kBPThreads) bp_kernel(BPParams bp, const BPVie
     const float bv = fmaf(m4, fi, fmaf(m5, fj, m7));
     const float bh = fmaf(m8, fi, fmaf(m9, fj, m11));
     SoftBil smp{spad + (int64_t)n * bp.sino_pad_elems, pu, mu, mv};
-#pragma unroll
-    for (int z = 0; z < kZC; ++z) {
-      const float fk = (float)(k0 + z);
-      const float h = fmaf(m10, fk, bh);
-      const float rh = __frcp_rn(h);
-      const float u = fmaf(m2, fk, bu) * rh;
-      const float v = fmaf(m6, fk, bv) * rh;
+    if constexpr (kZAff) {
+      const float rh = __frcp_rn(bh);
+      const float u = bu * rh, v0 = fmaf(m6, (float)k0, bv) * rh, dv = m6 * rh;
       float wgt = bp.scale;
       if (bp.power == 2) wgt *= rh * rh;
       else if (bp.power == 1) wgt *= rh;
-      if (bp.extent) {
-        const float tx = u + 0.5f, ty = v + 0.5f;
-        if (tx < -1.f || tx > bp.nx + 1.f || ty < -1.f || ty > bp.ny + 1.f) wgt = 0.f;
+      const bool col_out = bp.extent && (u + 0.5f < -1.f || u + 0.5f > bp.nx + 1.f);
+      if (col_out) continue;
+#pragma unroll
+      for (int z = 0; z < kZC; ++z) {
+        const float v = fmaf((float)z, dv, v0);
+        float wz = wgt;
+        if (bp.extent && (v + 0.5f < -1.f || v + 0.5f > bp.ny + 1.f)) wz = 0.f;
+        float val;
+        if constexpr (kTex) val = tex2DLayered<float>(tex, u + 0.5f, v + 0.5f, n);
+        else val = smp(u, v);
+        acc[z] = fmaf(val, wz, acc[z]);
       }
-      float val;
-      if constexpr (kTex) val = tex2DLayered<float>(tex, u + 0.5f, v + 0.5f, n);
-      else val = smp(u, v);
-      acc[z] = fmaf(val, wgt, acc[z]);
+    } else {
+#pragma unroll
+      for (int z = 0; z < kZC; ++z) {
+        const float fk = (float)(k0 + z);
+        const float h = fmaf(m10, fk, bh);
+        const float rh = __frcp_rn(h);
+        const float u = fmaf(m2, fk, bu) * rh;
+        const float v = fmaf(m6, fk, bv) * rh;
+        float wgt = bp.scale;
+        if (bp.power == 2) wgt *= rh * rh;
+        else if (bp.power == 1) wgt *= rh;
+        if (bp.extent) {
+          const float tx = u + 0.5f, ty = v + 0.5f;
+          if (tx < -1.f || tx > bp.nx + 1.f || ty < -1.f || ty > bp.ny + 1.f) wgt = 0.f;
+        }
+        float val;
+        if constexpr (kTex) val = tex2DLayered<float>(tex, u + 0.5f, v + 0.5f, n);
+        else val = smp(u, v);
+        acc[z] = fmaf(val, wgt, acc[z]);
+      }
     }
   }
   const int64_t plane = (int64_t)bp.nx * bp.ny;
@@ -140,16 +164,26 @@ int backward_impl(Plan* p, const float* sino, int batch, float* out, int accumul
       cp.extent = make_cudaExtent(gp.nu, gp.nv, gp.n_views);
       cp.kind = cudaMemcpyDeviceToDevice;
       DTV_CUDA_TRY(cudaMemcpy3DAsync(&cp, st));
-      bp_kernel<true><<<grid, kBPThreads, 0, st>>>(bp, p->d_bpv, nullptr, p->sino_tex[0],
-                                                   out + (int64_t)b * gp.nx * gp.ny * gp.nz,
-                                                   accumulate); note_launch();
+      float* ob = out + (int64_t)b * gp.nx * gp.ny * gp.nz;
+      if (p->bp_zaffine) {
+        bp_kernel<true, true><<<grid, kBPThreads, 0, st>>>(bp, p->d_bpv, nullptr, p->sino_tex[0],
+                                                           ob, accumulate); note_launch();
+      } else {
+        bp_kernel<true, false><<<grid, kBPThreads, 0, st>>>(bp, p->d_bpv, nullptr, p->sino_tex[0],
+                                                            ob, accumulate); note_launch();
+      }
     } else {
       stage_sino_pad_kernel<<<(int)std::min<int64_t>((per_item + 255) / 256, 148 * 16), 256, 0,
                               st>>>(sino + b * per_item, p->d_sino_pad, gp.nu, gp.nv, gp.n_views); note_launch();
       DTV_LAUNCH_CHECK();
-      bp_kernel<false><<<grid, kBPThreads, 0, st>>>(bp, p->d_bpv, p->d_sino_pad, 0,
-                                                    out + (int64_t)b * gp.nx * gp.ny * gp.nz,
-                                                    accumulate); note_launch();
+      float* ob = out + (int64_t)b * gp.nx * gp.ny * gp.nz;
+      if (p->bp_zaffine) {
+        bp_kernel<false, true><<<grid, kBPThreads, 0, st>>>(bp, p->d_bpv, p->d_sino_pad, 0, ob,
+                                                            accumulate); note_launch();
+      } else {
+        bp_kernel<false, false><<<grid, kBPThreads, 0, st>>>(bp, p->d_bpv, p->d_sino_pad, 0, ob,
+                                                             accumulate); note_launch();
+      }
     }
     DTV_LAUNCH_CHECK();
   }

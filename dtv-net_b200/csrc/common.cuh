@@ -127,11 +127,14 @@ struct Plan {
   cudaTextureObject_t* pair_tex;
   cudaSurfaceObject_t* pair_surf;
   cudaTextureObject_t* pair_tex_dev;
+  int fp_ray_tile;           // DTV_TUNE_FP_RAY_TILE
+  int bp_zaffine;            // every view's u and h are independent of z
   // adjoint ray table (DTV_PLAN_ADJOINT): per view and pixel, (p0, count) and (dp, 0)
   float4* d_rays;
   double fp_samples;  // per volume, < 0 until computed
 };
 
+constexpr int kNumRayTiles = 8;  // forward-projector ray tiles (DTV_TUNE_FP_RAY_TILE)
 constexpr int kPad = 2;  // zero border of the staged volume
 
 // kernels entry points used across units

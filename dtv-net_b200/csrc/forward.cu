@@ -27,6 +27,8 @@ struct RayParams {
   double voxel[3];
   double step;
   float scale;
+  // ray tile of a block (tu x tv pixels) and of a warp (wu x wv = 32), log2
+  int ltu, ltv, lwu;
 };
 
 static RayParams make_ray_params(const GeomParams& gp) {
@@ -37,6 +39,7 @@ static RayParams make_ray_params(const GeomParams& gp) {
   for (int c = 0; c < 3; ++c) r.voxel[c] = gp.voxel[c];
   r.step = gp.step;
   r.scale = (float)gp.scale;
+  r.ltu = 4; r.ltv = 4; r.lwu = 3;
   return r;
 }
 
@@ -188,14 +191,21 @@ struct FPOut {
   int epilogue;
 };
 
-constexpr int kTileU = 16, kTileV = 16, kFPThreads = kTileU * kTileV;
+constexpr int kFPThreads = 256;
 
-__device__ __forceinline__ void tile_pixel(int tiles_u, int& u, int& v) {
-  // 8 warps as 2 (u) x 4 (v); a warp covers 8 (u) x 4 (v) pixels
+// Ray tiles {log2 tu, log2 tv, log2 wu}: a block projects tu x tv detector
+// pixels of one view (tu * tv = 256), a warp wu x (32 / wu) of them. The shape
+// decides how compact each warp's texture footprint is.
+static const int kRayTiles[kNumRayTiles][3] = {{4, 4, 3}, {4, 4, 4}, {5, 3, 5}, {4, 4, 2},
+                                               {5, 3, 3}, {3, 5, 3}, {6, 2, 5}, {3, 5, 2}};
+
+__device__ __forceinline__ void tile_pixel(const RayParams& rp, int& u, int& v) {
   const int t = threadIdx.x, w = t >> 5, l = t & 31;
+  const int tiles_u = (rp.nu + (1 << rp.ltu) - 1) >> rp.ltu;
   const int tu = blockIdx.x % tiles_u, tv = blockIdx.x / tiles_u;
-  u = tu * kTileU + (w & 1) * 8 + (l & 7);
-  v = tv * kTileV + (w >> 1) * 4 + (l >> 3);
+  const int lwpr = rp.ltu - rp.lwu;  // log2 warps per tile row
+  u = (tu << rp.ltu) + ((w & ((1 << lwpr) - 1)) << rp.lwu) + (l & ((1 << rp.lwu) - 1));
+  v = (tv << rp.ltv) + ((w >> lwpr) << (5 - rp.lwu)) + (l >> rp.lwu);
 }
 
 __device__ __forceinline__ void block_add_double(double val, double* dst) {
@@ -240,9 +250,8 @@ template <class T>
 __global__ void __launch_bounds__(kFPThreads) fp_soft_kernel(RayParams rp, const FPView* __restrict__ views,
                                                              const T* __restrict__ vpad,
                                                              int64_t pad_elems, FPOut o) {
-  const int tiles_u = (rp.nu + kTileU - 1) / kTileU;
   int u, v;
-  tile_pixel(tiles_u, u, v);
+  tile_pixel(rp, u, v);
   const int n = blockIdx.y, b = blockIdx.z;
   float res = 0.f;
   const bool live = u < rp.nu && v < rp.nv;
@@ -269,9 +278,8 @@ __global__ void __launch_bounds__(kFPThreads) fp_soft_kernel(RayParams rp, const
 
 __global__ void __launch_bounds__(kFPThreads) fp_tex_kernel(RayParams rp, const FPView* __restrict__ views,
                                                             const cudaTextureObject_t* texs, FPOut o) {
-  const int tiles_u = (rp.nu + kTileU - 1) / kTileU;
   int u, v;
-  tile_pixel(tiles_u, u, v);
+  tile_pixel(rp, u, v);
   const int n = blockIdx.y, b = blockIdx.z;
   float res = 0.f;
   if (u < rp.nu && v < rp.nv) {
@@ -292,10 +300,10 @@ __global__ void __launch_bounds__(kFPThreads) fp_tex_kernel(RayParams rp, const 
 }
 
 __global__ void __launch_bounds__(kFPThreads) fp_pair_kernel(RayParams rp, const FPView* __restrict__ views,
-                                                             const cudaTextureObject_t* texs, FPOut o) {
-  const int tiles_u = (rp.nu + kTileU - 1) / kTileU;
+                                                             const cudaTextureObject_t* texs,
+                                                             FPOut o) {
   int u, v;
-  tile_pixel(tiles_u, u, v);
+  tile_pixel(rp, u, v);
   const int n = blockIdx.y, b = blockIdx.z;
   float res = 0.f;
   if (u < rp.nu && v < rp.nv) {
@@ -316,7 +324,8 @@ __global__ void __launch_bounds__(kFPThreads) fp_pair_kernel(RayParams rp, const
 }
 
 // Writes the z-pair layers of one volume: layer L = (f[L-2], f[L-1]), zero
-// outside [0, nz). One thread per (x, y) column walks the nz + 3 layers.
+// outside [0, nz), to the layered texture. One thread per (x, y) column walks
+// the nz + 3 layers.
 template <class Tin>
 __global__ void __launch_bounds__(256) stage_pairs_kernel(const Tin* __restrict__ in,
                                                           cudaSurfaceObject_t surf, int nx, int ny,
@@ -451,8 +460,11 @@ int forward_impl(Plan* p, const void* vol, int vol_dtype, int batch, float* out,
   }
   if (rc) return rc;
   RayParams rp = make_ray_params(gp);
+  rp.ltu = kRayTiles[p->fp_ray_tile][0];
+  rp.ltv = kRayTiles[p->fp_ray_tile][1];
+  rp.lwu = kRayTiles[p->fp_ray_tile][2];
   FPOut o{out, g, sigma, abs_sum, epilogue};
-  const int tiles = ((gp.nu + kTileU - 1) / kTileU) * ((gp.nv + kTileV - 1) / kTileV);
+  const int tiles = ((gp.nu + (1 << rp.ltu) - 1) >> rp.ltu) * ((gp.nv + (1 << rp.ltv) - 1) >> rp.ltv);
   dim3 grid(tiles, gp.n_views, batch);
   if (pairs) {
     fp_pair_kernel<<<grid, kFPThreads, 0, st>>>(rp, p->d_fpv, p->pair_tex_dev, o); note_launch();

@@ -110,6 +110,9 @@ int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Pla
     return rc;
   }
   const GeomParams& gp = p->gp;
+  p->bp_zaffine = 1;
+  for (int n = 0; n < gp.n_views; ++n)
+    if (bpv[n].m[2] != 0.f || bpv[n].m[10] != 0.f) p->bp_zaffine = 0;
 #define PLAN_CUDA(expr)                                                                  \
   do {                                                                                   \
     cudaError_t _e = (expr);                                                             \
@@ -262,6 +265,32 @@ int dtv_plan_destroy(dtv_plan* plan) {
   DeviceGuard dg(p->device);
   free_plan(p);
   return DTV_OK;
+}
+
+int dtv_plan_set_tuning(dtv_plan* plan, int32_t key, int32_t value) {
+  DTV_CHECK(plan != nullptr, "plan is NULL");
+  Plan* p = reinterpret_cast<Plan*>(plan);
+  switch (key) {
+    case DTV_TUNE_FP_RAY_TILE:
+      DTV_CHECK(value >= 0 && value < kNumRayTiles, "DTV_TUNE_FP_RAY_TILE must be in [0, %d]",
+                kNumRayTiles - 1);
+      p->fp_ray_tile = value;
+      return DTV_OK;
+    default:
+      return fail(DTV_ERR_INVALID, "unknown tuning key %d", key);
+  }
+}
+
+int dtv_plan_get_tuning(const dtv_plan* plan, int32_t key, int32_t* value) {
+  DTV_CHECK(plan && value, "NULL argument");
+  const Plan* p = reinterpret_cast<const Plan*>(plan);
+  switch (key) {
+    case DTV_TUNE_FP_RAY_TILE:
+      *value = p->fp_ray_tile;
+      return DTV_OK;
+    default:
+      return fail(DTV_ERR_INVALID, "unknown tuning key %d", key);
+  }
 }
 
 int dtv_plan_fp_samples(const dtv_plan* plan, double* samples) {

@@ -3,7 +3,7 @@
 The compute path is the sm_100a kernel library libdtvb200.so behind the C ABI
 of include/dtv_b200.h; this package is its host side. There is no CPU path.
 """
-from . import _lib
+from . import _lib, autotune
 from ._lib import DtvError
 from .geometry import Geometry, Plan, circular, standard, vector
 from .ops import (BeijingGeometry, Projector, StandardGeometry, StandardGeometryWithFBP,

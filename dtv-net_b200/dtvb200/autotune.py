@@ -1,0 +1,77 @@
+"""Launch-parameter autotuner for projector plans.
+
+A plan's tuning keys (DTV_TUNE_*) change how its kernels are launched, not
+what they compute (beyond FP32 rounding). ``tune`` times each candidate value
+of a key on the plan's own geometry with CUDA events, keeps the fastest, and
+remembers the choice per (device, geometry, batch, key) for the rest of the
+process, so plans created later for the same workload reuse it without timing.
+
+DTV_TUNE_FP_RAY_TILE picks the forward projector's ray tile: which detector
+pixels share a block (256 rays of one view) and a warp (32 rays). The samplers
+are bound by the texture / L1 pipe, whose throughput depends on how many cache
+lines the 32 samples of one warp instruction touch, and that depends on the
+tile and on the geometry (magnification, pixel pitch, volume aspect).
+"""
+from __future__ import annotations
+
+import torch
+
+from . import _lib
+from .geometry import Plan
+
+_CACHE: dict = {}
+N_RAY_TILES = 8
+
+
+def _key(plan: Plan, batch: int, key: int):
+    return (torch.cuda.get_device_name(plan.device), plan.sampler, int(batch),
+            plan.geometry.key(), int(key))
+
+
+def time_forward(plan: Plan, vol: torch.Tensor, out: torch.Tensor, reps: int = 5,
+                 warmup: int = 2) -> float:
+    """Median milliseconds of ``plan.forward(vol, out)`` on the current stream."""
+    with torch.cuda.device(plan.device):
+        for _ in range(warmup):
+            plan.forward(vol, out)
+        times = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            plan.forward(vol, out)
+            b.record()
+            b.synchronize()
+            times.append(a.elapsed_time(b))
+    times.sort()
+    return times[len(times) // 2]
+
+
+def tune(plan: Plan, batch: int = 1, key: int = _lib.DTV_TUNE_FP_RAY_TILE, candidates=None,
+         reps: int = 5, warmup: int = 2, use_cache: bool = True) -> dict:
+    """Time ``candidates`` for ``key`` on ``plan`` and set the fastest.
+
+    Returns {value: milliseconds}. A cached choice is applied without
+    timing."""
+    if key != _lib.DTV_TUNE_FP_RAY_TILE:
+        raise ValueError(f"unknown tuning key {key}")
+    ck = _key(plan, batch, key)
+    if use_cache and ck in _CACHE:
+        plan.set_tuning(key, _CACHE[ck][0])
+        return dict(_CACHE[ck][1])
+    if candidates is None:
+        candidates = range(N_RAY_TILES)
+    gen = torch.Generator(device=plan.device).manual_seed(0)
+    vol = torch.rand(plan.vol_shape(batch), device=plan.device, generator=gen)
+    out = torch.empty(plan.sino_shape(batch), device=plan.device)
+    times = {}
+    for c in candidates:
+        plan.set_tuning(key, int(c))
+        times[int(c)] = time_forward(plan, vol, out, reps, warmup)
+    best = min(times, key=times.get)
+    plan.set_tuning(key, best)
+    _CACHE[ck] = (best, dict(times))
+    return times
+
+
+def clear_cache() -> None:
+    _CACHE.clear()

@@ -169,6 +169,17 @@ class Plan:
     def sino_shape(self, batch: int = 1):
         return self.geometry.sino_shape(batch)
 
+    def set_tuning(self, key: int, value: int) -> None:
+        """Set a launch parameter (DTV_TUNE_*); results do not depend on it.
+        DTV_TUNE_FP_RAY_TILE (0..7): the forward projector's block and warp
+        ray tile, which decides how compact each warp's texture footprint is."""
+        call("dtv_plan_set_tuning", self._h, int(key), int(value))
+
+    def get_tuning(self, key: int) -> int:
+        out = ctypes.c_int32()
+        call("dtv_plan_get_tuning", self._h, int(key), ctypes.byref(out))
+        return out.value
+
     def fp_samples(self) -> float:
         """Forward-projector samples per volume (exact chords / step)."""
         out = ctypes.c_double()

@@ -160,6 +160,16 @@ DTV_API int dtv_geometry_circular(dtv_geometry* g, double* views, const double* 
 DTV_API int dtv_plan_create(const dtv_geometry* g, int32_t max_batch, int32_t flags, int32_t device,
                     dtv_plan** out);
 DTV_API int dtv_plan_destroy(dtv_plan* plan);
+/* Launch knobs of a plan, set by an autotuner that times the candidates; the
+ * results do not depend on them (each ray's sum is the same computation):
+ *   DTV_TUNE_FP_RAY_TILE: the forward projector's ray tile, 0..7, as
+ *   (block tu x tv pixels, warp wu x wv pixels): 0 (16x16, 8x4) default,
+ *   1 (16x16, 16x2), 2 (32x8, 32x1), 3 (16x16, 4x8), 4 (32x8, 8x4),
+ *   5 (8x32, 8x4), 6 (64x4, 32x1), 7 (8x32, 4x8).
+ * No counterpart in the reference (its kernels use one fixed launch shape). */
+#define DTV_TUNE_FP_RAY_TILE 1
+DTV_API int dtv_plan_set_tuning(dtv_plan* plan, int32_t key, int32_t value);
+DTV_API int dtv_plan_get_tuning(const dtv_plan* plan, int32_t key, int32_t* value);
 /* Number of forward-projector ray samples per volume (exact chord count under
  * the plan's phase rule, the algorithmic work unit), computed on the host. */
 DTV_API int dtv_plan_fp_samples(const dtv_plan* plan, double* samples_per_volume);

@@ -87,6 +87,39 @@ def test_forward_pairs_matches_oracle(cuda, kind):
     assert rel_rmse(out, O.forward(og, vol).reshape(out.shape)) < 1e-3
 
 
+@pytest.mark.parametrize("sampler", ["soft", "tex", "pairs"])
+def test_forward_ray_tiles_agree(cuda, sampler):
+    """Every ray tile computes the same per-ray sums (bit-identical), with
+    detector sizes that leave partial tiles in u and v."""
+    g, og = make_case("standard_odd")
+    plan = dtvb200.Plan(g, max_batch=2, sampler=sampler, device=cuda)
+    vol = to_dev(blob_volume(np.random.default_rng(22), og.vol_shape, 2), cuda)
+    key = _lib.DTV_TUNE_FP_RAY_TILE
+    assert plan.get_tuning(key) == 0
+    ref = plan.forward(vol).clone()
+    for t in range(1, dtvb200.autotune.N_RAY_TILES):
+        plan.set_tuning(key, t)
+        assert torch.equal(plan.forward(vol), ref), t
+
+
+def test_tuning_keys_and_autotune(cuda):
+    g, og = make_case("standard")
+    plan = dtvb200.Plan(g, sampler="pairs", device=cuda)
+    key = _lib.DTV_TUNE_FP_RAY_TILE
+    for bad in (-1, dtvb200.autotune.N_RAY_TILES):
+        with pytest.raises(dtvb200.DtvError):
+            plan.set_tuning(key, bad)
+    with pytest.raises(dtvb200.DtvError):
+        plan.set_tuning(99, 0)
+    dtvb200.autotune.clear_cache()
+    times = dtvb200.autotune.tune(plan, reps=3, warmup=1)
+    assert sorted(times) == list(range(dtvb200.autotune.N_RAY_TILES))
+    assert plan.get_tuning(key) == min(times, key=times.get)
+    other = dtvb200.Plan(g, sampler="pairs", device=cuda)
+    assert dtvb200.autotune.tune(other) == times  # cached: applied without timing
+    assert other.get_tuning(key) == plan.get_tuning(key)
+
+
 @pytest.mark.parametrize("kind", KINDS)
 @pytest.mark.parametrize("sampler", ["soft", "tex", "pairs"])
 def test_backward_fdk_matches_oracle(cuda, kind, sampler):
