@@ -128,6 +128,14 @@ struct Plan {
   cudaSurfaceObject_t* pair_surf;
   cudaTextureObject_t* pair_tex_dev;
   int fp_ray_tile;           // DTV_TUNE_FP_RAY_TILE
+  // shared-memory staged forward projector (DTV_PLAN_TMA): the z pairs as a
+  // linear [batch][nz+3][ny][pair_pitch] u32 array and its two tensor maps
+  // (boxes for chunks along x and along y)
+  unsigned int* d_pair_lin;
+  int pair_pitch;
+  int fp_tex_share;          // DTV_TUNE_FP_TEX_SHARE
+  alignas(64) unsigned char tmap[2][128];
+  int* d_status;             // device error bits
   int bp_zaffine;            // every view's u and h are independent of z
   // adjoint ray table (DTV_PLAN_ADJOINT): per view and pixel, (p0, count) and (dp, 0)
   float4* d_rays;
@@ -143,6 +151,7 @@ int forward_impl(Plan* p, const void* vol, int vol_dtype, int batch, float* out,
 int backward_impl(Plan* p, const float* sino, int batch, float* out, int accumulate,
                   cudaStream_t st);
 int adjoint_impl(Plan* p, const float* sino, int batch, float* out, cudaStream_t st);
+int encode_pair_maps(Plan* p);
 int build_ray_table(Plan* p, cudaStream_t st);
 
 }  // namespace dtv

@@ -17,125 +17,9 @@
 #include <algorithm>
 #include <string.h>
 
-#include "common.cuh"
+#include "ray.cuh"
 
 namespace dtv {
-
-struct RayParams {
-  int nx, ny, nz, nu, nv, n_views;
-  int phase;
-  double voxel[3];
-  double step;
-  float scale;
-  // ray tile of a block (tu x tv pixels) and of a warp (wu x wv = 32), log2
-  int ltu, ltv, lwu;
-};
-
-static RayParams make_ray_params(const GeomParams& gp) {
-  RayParams r;
-  r.nx = gp.nx; r.ny = gp.ny; r.nz = gp.nz;
-  r.nu = gp.nu; r.nv = gp.nv; r.n_views = gp.n_views;
-  r.phase = gp.phase;
-  for (int c = 0; c < 3; ++c) r.voxel[c] = gp.voxel[c];
-  r.step = gp.step;
-  r.scale = (float)gp.scale;
-  r.ltu = 4; r.ltv = 4; r.lwu = 3;
-  return r;
-}
-
-// Per-ray set-up: the first sample position and step (index space) and the
-// number of samples that can be non-zero.
-struct RaySetup {
-  float p0[3];
-  float dp[3];
-  int count;
-};
-
-// `sxy` / `sz` are added to the start position's x,y / z (1/2 where the
-// sampler takes texture coordinates, whose texel centres sit at i + 1/2).
-__device__ __forceinline__ RaySetup setup_ray(const RayParams& rp, const FPView& f, int u, int v,
-                                              float sxy = 0.f, float sz = 0.f) {
-  RaySetup rs;
-  double r[3], rw[3];
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    r[c] = f.d0ms[c] + u * f.u[c] + v * f.v[c];
-    rw[c] = r[c] * rp.voxel[c];
-  }
-  const double inv = rsqrt(rw[0] * rw[0] + rw[1] * rw[1] + rw[2] * rw[2]);
-  double d[3], dw[3];
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    d[c] = r[c] * inv;    // index units per world unit of alpha
-    dw[c] = rw[c] * inv;  // unit world direction
-  }
-  const int n3[3] = {rp.nx, rp.ny, rp.nz};
-  double a0;
-  double ktot;
-  if (rp.phase == DTV_PHASE_BOX) {
-    double lo = -1e300, hi = 1e300;
-    bool miss = false;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      if (d[c] == 0.0) {
-        if (f.s[c] < -0.5 || f.s[c] > n3[c] - 0.5) miss = true;
-      } else {
-        double t0 = (-0.5 - f.s[c]) / d[c], t1 = (n3[c] - 0.5 - f.s[c]) / d[c];
-        lo = fmax(lo, fmin(t0, t1));
-        hi = fmin(hi, fmax(t0, t1));
-      }
-    }
-    if (miss || !(hi > lo)) {
-      rs.count = 0;
-      return rs;
-    }
-    ktot = ceil((hi - lo) / rp.step);
-    a0 = lo + 0.5 * rp.step;
-  } else {
-    int ax;
-    if (rp.phase == DTV_PHASE_STANDARD) {
-      ax = fabs(dw[0]) >= fabs(dw[1]) ? 0 : 1;  // Standard forwardKernel.cu:45
-    } else {                                    // Beijing forwardKernel.cu:40-58
-      const double dom = fmax(fabs(dw[0]), fmax(fabs(dw[2]), fabs(dw[1])));
-      ax = fabs(dw[0]) == dom ? 0 : (fabs(dw[1]) == dom ? 1 : 2);
-    }
-    // bounds +-n/2 in WORLD units against the world source (the reference's
-    // alpha range, forwardKernel.cu:46-58)
-    const double e = n3[ax] * 0.5;
-    const double t0 = (-e - f.sw[ax]) / dw[ax], t1 = (e - f.sw[ax]) / dw[ax];
-    const double lo = fmin(t0, t1) - 3.0, hi = fmax(t0, t1) + 3.0;
-    a0 = lo;
-    ktot = ceil((hi - lo) / rp.step);
-  }
-  // clip k to samples whose position lies in (-1, n) on every axis
-  double klo = 0.0, khi = ktot;
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    const double base = f.s[c] + a0 * d[c];
-    const double dc = d[c] * rp.step;
-    if (fabs(dc) < 1e-12) {
-      if (base <= -1.0 || base >= n3[c]) khi = -1.0;
-    } else {
-      const double ka = (-1.0 - base) / dc, kb = (n3[c] - base) / dc;
-      klo = fmax(klo, fmin(ka, kb));
-      khi = fmin(khi, fmax(ka, kb));
-    }
-  }
-  const double kb = fmax(floor(klo), 0.0);
-  const double ke = fmin(ceil(khi) + 1.0, ktot);
-  if (!(ke > kb)) {
-    rs.count = 0;
-    return rs;
-  }
-  rs.count = (int)(ke - kb);
-  const double ab = a0 + kb * rp.step;
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    rs.p0[c] = (float)(f.s[c] + ab * d[c] + (c < 2 ? sxy : sz));
-    rs.dp[c] = (float)(d[c] * rp.step);
-  }
-  return rs;
-}
 
 // ---- samplers --------------------------------------------------------------------------
 template <class T>
@@ -169,29 +53,6 @@ struct TexSampler {
   }
 };
 
-// z-pair sampler: layer L of the half2 layered texture holds (f[L-2], f[L-1]).
-// x, y arrive as texture coordinates (shifted by 1/2), z as a voxel index.
-struct PairSampler {
-  cudaTextureObject_t tex;
-  float lmax;  // nz + 2, the last layer
-  __device__ __forceinline__ float operator()(float x, float y, float z) const {
-    const float fz = floorf(z);
-    const float w = z - fz;
-    const float L = fminf(fmaxf(fz + 2.f, 0.f), lmax);
-    const float2 a = tex2DLayered<float2>(tex, x, y, (int)L);
-    return fmaf(w, a.y - a.x, a.x);
-  }
-};
-
-struct FPOut {
-  float* out;
-  const float* g;
-  float sigma;
-  double* abs_sum;
-  int epilogue;
-};
-
-constexpr int kFPThreads = 256;
 
 // Ray tiles {log2 tu, log2 tv, log2 wu}: a block projects tu x tv detector
 // pixels of one view (tu * tv = 256), a warp wu x (32 / wu) of them. The shape
@@ -206,44 +67,6 @@ __device__ __forceinline__ void tile_pixel(const RayParams& rp, int& u, int& v) 
   const int lwpr = rp.ltu - rp.lwu;  // log2 warps per tile row
   u = (tu << rp.ltu) + ((w & ((1 << lwpr) - 1)) << rp.lwu) + (l & ((1 << rp.lwu) - 1));
   v = (tv << rp.ltv) + ((w >> lwpr) << (5 - rp.lwu)) + (l >> rp.lwu);
-}
-
-__device__ __forceinline__ void block_add_double(double val, double* dst) {
-  __shared__ double red[kFPThreads / 32];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = val;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int i = 0; i < kFPThreads / 32; ++i) s += red[i];
-    if (s != 0.0) atomicAdd(dst, s);
-  }
-}
-
-template <class Sampler>
-__device__ __forceinline__ float ray_sum(const Sampler& smp, const RaySetup& rs) {
-  float a0 = 0.f, a1 = 0.f;
-  int k = 0;
-  for (; k + 3 < rs.count; k += 4) {
-    float s[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const float kf = (float)(k + j);
-      s[j] = smp(fmaf(kf, rs.dp[0], rs.p0[0]), fmaf(kf, rs.dp[1], rs.p0[1]),
-                 fmaf(kf, rs.dp[2], rs.p0[2]));
-    }
-    a0 += s[0];
-    a1 += s[1];
-    a0 += s[2];
-    a1 += s[3];
-  }
-  for (; k < rs.count; ++k) {
-    const float kf = (float)k;
-    a0 += smp(fmaf(kf, rs.dp[0], rs.p0[0]), fmaf(kf, rs.dp[1], rs.p0[1]),
-              fmaf(kf, rs.dp[2], rs.p0[2]));
-  }
-  return a0 + a1;
 }
 
 template <class T>
@@ -263,15 +86,7 @@ __global__ void __launch_bounds__(kFPThreads) fp_soft_kernel(RayParams rp, const
     smp.pxy = smp.px * (rp.ny + 2 * kPad);
     smp.mx = (float)rp.nx; smp.my = (float)rp.ny; smp.mz = (float)rp.nz;
     const float val = rs.count > 0 ? ray_sum(smp, rs) * rp.scale : 0.f;
-    const int64_t idx = ((int64_t)b * rp.n_views + n) * rp.nu * rp.nv + (int64_t)v * rp.nu + u;
-    if (o.epilogue == DTV_EPI_STORE) {
-      o.out[idx] = val;
-      res = val;
-    } else {
-      res = val - o.g[idx];
-      if (o.epilogue == DTV_EPI_RESIDUAL) o.out[idx] = res;
-      else o.out[idx] = (o.out[idx] + o.sigma * res) / (1.f + o.sigma);
-    }
+    fp_store(rp, o, n, b, u, v, val, res);
   }
   if (o.abs_sum) block_add_double((double)fabsf(res), o.abs_sum);
 }
@@ -286,15 +101,7 @@ __global__ void __launch_bounds__(kFPThreads) fp_tex_kernel(RayParams rp, const 
     const RaySetup rs = setup_ray(rp, views[n], u, v, 0.5f, 0.5f);
     TexSampler smp{texs[b]};
     const float val = rs.count > 0 ? ray_sum(smp, rs) * rp.scale : 0.f;
-    const int64_t idx = ((int64_t)b * rp.n_views + n) * rp.nu * rp.nv + (int64_t)v * rp.nu + u;
-    if (o.epilogue == DTV_EPI_STORE) {
-      o.out[idx] = val;
-      res = val;
-    } else {
-      res = val - o.g[idx];
-      if (o.epilogue == DTV_EPI_RESIDUAL) o.out[idx] = res;
-      else o.out[idx] = (o.out[idx] + o.sigma * res) / (1.f + o.sigma);
-    }
+    fp_store(rp, o, n, b, u, v, val, res);
   }
   if (o.abs_sum) block_add_double((double)fabsf(res), o.abs_sum);
 }
@@ -310,26 +117,20 @@ __global__ void __launch_bounds__(kFPThreads) fp_pair_kernel(RayParams rp, const
     const RaySetup rs = setup_ray(rp, views[n], u, v, 0.5f, 0.f);
     PairSampler smp{texs[b], (float)(rp.nz + 2)};
     const float val = rs.count > 0 ? ray_sum(smp, rs) * rp.scale : 0.f;
-    const int64_t idx = ((int64_t)b * rp.n_views + n) * rp.nu * rp.nv + (int64_t)v * rp.nu + u;
-    if (o.epilogue == DTV_EPI_STORE) {
-      o.out[idx] = val;
-      res = val;
-    } else {
-      res = val - o.g[idx];
-      if (o.epilogue == DTV_EPI_RESIDUAL) o.out[idx] = res;
-      else o.out[idx] = (o.out[idx] + o.sigma * res) / (1.f + o.sigma);
-    }
+    fp_store(rp, o, n, b, u, v, val, res);
   }
   if (o.abs_sum) block_add_double((double)fabsf(res), o.abs_sum);
 }
 
 // Writes the z-pair layers of one volume: layer L = (f[L-2], f[L-1]), zero
-// outside [0, nz), to the layered texture. One thread per (x, y) column walks
-// the nz + 3 layers.
+// outside [0, nz), to the layered texture and, when `lin` is set, to the
+// linear [nz+3][ny][pitch] copy. One thread per (x, y) column walks the
+// nz + 3 layers.
 template <class Tin>
 __global__ void __launch_bounds__(256) stage_pairs_kernel(const Tin* __restrict__ in,
-                                                          cudaSurfaceObject_t surf, int nx, int ny,
-                                                          int nz) {
+                                                          cudaSurfaceObject_t surf,
+                                                          unsigned int* __restrict__ lin, int pitch,
+                                                          int nx, int ny, int nz) {
   const int x = blockIdx.x * 32 + (threadIdx.x & 31);
   const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
   if (x >= nx || y >= ny) return;
@@ -343,6 +144,7 @@ __global__ void __launch_bounds__(256) stage_pairs_kernel(const Tin* __restrict_
     const unsigned int bits = (unsigned int)__half_as_ushort(prev) |
                               ((unsigned int)__half_as_ushort(cur) << 16);
     surf2DLayeredwrite(bits, surf, x * 4, y, L);
+    if (lin) lin[((int64_t)L * ny + y) * pitch + x] = bits;
     prev = cur;
   }
 }
@@ -428,8 +230,10 @@ static int stage_volume_pairs(Plan* p, const Tin* vol, int batch, cudaStream_t s
   const int64_t vox = (int64_t)g.nx * g.ny * g.nz;
   dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8);
   for (int b = 0; b < batch; ++b) {
-    stage_pairs_kernel<Tin><<<grid, 256, 0, st>>>(vol + b * vox, p->pair_surf[b], g.nx, g.ny,
-                                                  g.nz); note_launch();
+    unsigned int* lin =
+        p->d_pair_lin ? p->d_pair_lin + (int64_t)b * p->pair_pitch * g.ny * (g.nz + 3) : nullptr;
+    stage_pairs_kernel<Tin><<<grid, 256, 0, st>>>(vol + b * vox, p->pair_surf[b], lin,
+                                                  p->pair_pitch, g.nx, g.ny, g.nz); note_launch();
     DTV_LAUNCH_CHECK();
   }
   return DTV_OK;
@@ -466,7 +270,9 @@ int forward_impl(Plan* p, const void* vol, int vol_dtype, int batch, float* out,
   FPOut o{out, g, sigma, abs_sum, epilogue};
   const int tiles = ((gp.nu + (1 << rp.ltu) - 1) >> rp.ltu) * ((gp.nv + (1 << rp.ltv) - 1) >> rp.ltv);
   dim3 grid(tiles, gp.n_views, batch);
-  if (pairs) {
+  if (p->flags & DTV_PLAN_TMA) {
+    return fp_tma_launch(p, rp, o, batch, st);
+  } else if (pairs) {
     fp_pair_kernel<<<grid, kFPThreads, 0, st>>>(rp, p->d_fpv, p->pair_tex_dev, o); note_launch();
   } else if (tex) {
     fp_tex_kernel<<<grid, kFPThreads, 0, st>>>(rp, p->d_fpv, p->vol_tex_dev, o); note_launch();

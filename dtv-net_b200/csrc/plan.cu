@@ -53,6 +53,8 @@ void free_plan(Plan* p) {
   free(p->sino_arrays);
   cudaFree(p->vol_tex_dev);
   cudaFree(p->d_rays);
+  cudaFree(p->d_pair_lin);
+  cudaFree(p->d_status);
   cudaFree(p->d_fpv);
   cudaFree(p->d_bpv);
   cudaFree(p->d_vol_pad);
@@ -80,7 +82,10 @@ int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Pla
   DTV_CHECK(out != nullptr, "out is NULL");
   *out = nullptr;
   DTV_CHECK(max_batch > 0, "max_batch must be positive");
-  DTV_CHECK((flags & ~(DTV_PLAN_TEX | DTV_PLAN_STAGE_F16 | DTV_PLAN_TEX_PAIRS | DTV_PLAN_ADJOINT)) ==
+  DTV_CHECK(!(flags & DTV_PLAN_TMA) || (flags & DTV_PLAN_TEX_PAIRS),
+            "DTV_PLAN_TMA needs DTV_PLAN_TEX_PAIRS");
+  DTV_CHECK((flags & ~(DTV_PLAN_TEX | DTV_PLAN_STAGE_F16 | DTV_PLAN_TEX_PAIRS | DTV_PLAN_ADJOINT |
+                       DTV_PLAN_TMA)) ==
                 0,
             "unknown plan flags 0x%x", flags);
   DTV_CHECK(!((flags & DTV_PLAN_TEX) && (flags & DTV_PLAN_TEX_PAIRS)),
@@ -201,6 +206,20 @@ int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Pla
     PLAN_CUDA(cudaMemcpy(p->pair_tex_dev, p->pair_tex, sizeof(cudaTextureObject_t) * max_batch,
                          cudaMemcpyHostToDevice));
   }
+  PLAN_CUDA(cudaMalloc(&p->d_status, sizeof(int)));
+  PLAN_CUDA(cudaMemset(p->d_status, 0, sizeof(int)));
+  if (flags & DTV_PLAN_TMA) {
+    p->pair_pitch = (gp.nx + 3) & ~3;  // rows of whole 16-byte units
+    const size_t words = (size_t)p->pair_pitch * gp.ny * (gp.nz + 3) * max_batch;
+    PLAN_CUDA(cudaMalloc(&p->d_pair_lin, words * sizeof(unsigned int)));
+    PLAN_CUDA(cudaMemset(p->d_pair_lin, 0, words * sizeof(unsigned int)));
+    p->fp_tex_share = 0;
+    rc = encode_pair_maps(p);
+    if (rc) {
+      free_plan(p);
+      return rc;
+    }
+  }
   if ((flags & (DTV_PLAN_TEX | DTV_PLAN_TEX_PAIRS)) && gp.n_views <= max_layers) {
     // backprojector: the sinogram as a layered texture (one layer per view);
     // with more views than layers the backprojector samples in software
@@ -271,6 +290,11 @@ int dtv_plan_set_tuning(dtv_plan* plan, int32_t key, int32_t value) {
   DTV_CHECK(plan != nullptr, "plan is NULL");
   Plan* p = reinterpret_cast<Plan*>(plan);
   switch (key) {
+    case DTV_TUNE_FP_TEX_SHARE:
+      DTV_CHECK(p->flags & DTV_PLAN_TMA, "DTV_TUNE_FP_TEX_SHARE needs a DTV_PLAN_TMA plan");
+      DTV_CHECK(value >= 0 && value <= 8, "DTV_TUNE_FP_TEX_SHARE must be in [0, 8]");
+      p->fp_tex_share = value;
+      return DTV_OK;
     case DTV_TUNE_FP_RAY_TILE:
       DTV_CHECK(value >= 0 && value < kNumRayTiles, "DTV_TUNE_FP_RAY_TILE must be in [0, %d]",
                 kNumRayTiles - 1);
@@ -288,9 +312,25 @@ int dtv_plan_get_tuning(const dtv_plan* plan, int32_t key, int32_t* value) {
     case DTV_TUNE_FP_RAY_TILE:
       *value = p->fp_ray_tile;
       return DTV_OK;
+    case DTV_TUNE_FP_TEX_SHARE:
+      *value = p->fp_tex_share;
+      return DTV_OK;
     default:
       return fail(DTV_ERR_INVALID, "unknown tuning key %d", key);
   }
+}
+
+int dtv_plan_device_status(dtv_plan* plan, int32_t* status, int32_t reset) {
+  DTV_CHECK(plan && status, "NULL argument");
+  Plan* p = reinterpret_cast<Plan*>(plan);
+  DeviceGuard dg(p->device);
+  if (!dg.ok) return fail(DTV_ERR_CUDA, "cannot select device %d", p->device);
+  int v = 0;
+  DTV_CUDA_TRY(cudaDeviceSynchronize());
+  DTV_CUDA_TRY(cudaMemcpy(&v, p->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (reset) DTV_CUDA_TRY(cudaMemset(p->d_status, 0, sizeof(int)));
+  *status = v;
+  return DTV_OK;
 }
 
 int dtv_plan_fp_samples(const dtv_plan* plan, double* samples) {

@@ -16,7 +16,9 @@ DTV_F32, DTV_F16, DTV_BF16 = 0, 1, 2
 DTV_PHASE_STANDARD, DTV_PHASE_VECTOR, DTV_PHASE_BOX = 0, 1, 2
 DTV_PLAN_SOFT, DTV_PLAN_TEX, DTV_PLAN_STAGE_F16, DTV_PLAN_TEX_PAIRS = 0x0, 0x1, 0x2, 0x4
 DTV_PLAN_ADJOINT = 0x8
+DTV_PLAN_TMA = 0x10
 DTV_TUNE_FP_RAY_TILE = 1
+DTV_TUNE_FP_TEX_SHARE = 2
 DTV_EPI_STORE, DTV_EPI_RESIDUAL, DTV_EPI_PDHG = 0, 1, 2
 
 
@@ -72,6 +74,7 @@ SIGNATURES = {
     "dtv_plan_destroy": [_P],
     "dtv_plan_set_tuning": [_P, _I, _I],
     "dtv_plan_get_tuning": [_P, _I, _IP],
+    "dtv_plan_device_status": [_P, _IP, _I],
     "dtv_plan_fp_samples": [_P, _DP],
     "dtv_forward": [_P, _P, _I, _I, _P, _I, _P, _F, _P, _P],
     "dtv_backward": [_P, _P, _I, _P, _I, _P],

@@ -11,6 +11,10 @@ pixels share a block (256 rays of one view) and a warp (32 rays). The samplers
 are bound by the texture / L1 pipe, whose throughput depends on how many cache
 lines the 32 samples of one warp instruction touch, and that depends on the
 tile and on the geometry (magnification, pixel pitch, volume aspect).
+
+DTV_TUNE_FP_TEX_SHARE applies to "tma" plans: of every 8 ray tiles, that
+many sample through the texture unit and the rest from shared memory, so the
+texture pipe and the shared-memory/FMA pipes work side by side.
 """
 from __future__ import annotations
 
@@ -21,6 +25,7 @@ from .geometry import Plan
 
 _CACHE: dict = {}
 N_RAY_TILES = 8
+CANDIDATES = {_lib.DTV_TUNE_FP_RAY_TILE: range(N_RAY_TILES), _lib.DTV_TUNE_FP_TEX_SHARE: range(9)}
 
 
 def _key(plan: Plan, batch: int, key: int):
@@ -46,20 +51,24 @@ def time_forward(plan: Plan, vol: torch.Tensor, out: torch.Tensor, reps: int = 5
     return times[len(times) // 2]
 
 
-def tune(plan: Plan, batch: int = 1, key: int = _lib.DTV_TUNE_FP_RAY_TILE, candidates=None,
+def tune(plan: Plan, batch: int = 1, key: int = None, candidates=None,
          reps: int = 5, warmup: int = 2, use_cache: bool = True) -> dict:
     """Time ``candidates`` for ``key`` on ``plan`` and set the fastest.
 
+    ``key`` defaults to the key that applies to the plan's sampler
+    (DTV_TUNE_FP_TEX_SHARE for "tma", DTV_TUNE_FP_RAY_TILE otherwise).
     Returns {value: milliseconds}. A cached choice is applied without
     timing."""
-    if key != _lib.DTV_TUNE_FP_RAY_TILE:
+    if key is None:
+        key = _lib.DTV_TUNE_FP_TEX_SHARE if plan.sampler == "tma" else _lib.DTV_TUNE_FP_RAY_TILE
+    if key not in CANDIDATES:
         raise ValueError(f"unknown tuning key {key}")
     ck = _key(plan, batch, key)
     if use_cache and ck in _CACHE:
         plan.set_tuning(key, _CACHE[ck][0])
         return dict(_CACHE[ck][1])
     if candidates is None:
-        candidates = range(N_RAY_TILES)
+        candidates = CANDIDATES[key]
     gen = torch.Generator(device=plan.device).manual_seed(0)
     vol = torch.rand(plan.vol_shape(batch), device=plan.device, generator=gen)
     out = torch.empty(plan.sino_shape(batch), device=plan.device)

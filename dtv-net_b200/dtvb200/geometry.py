@@ -130,21 +130,27 @@ def check_input(t: torch.Tensor, name: str, shape=None, dtypes=(torch.float32,))
         raise RuntimeError(f"{name} must have shape {tuple(shape)}, got {tuple(t.shape)}")
 
 
+SAMPLERS = ("soft", "tex", "pairs", "tma")
+
+
 class Plan:
     """A geometry uploaded to one GPU with sampler staging for ``max_batch``
     volumes. ``sampler``: "soft" (software trilinear, FP32 weights; required
     for the exact adjoint), "tex" (hardware trilinear texture filtering, like
     the reference) or "pairs" (FP16 z-plane pairs in a layered texture: one
-    bilinear fetch per sample, z interpolated in FP32). The backprojector
-    samples the sinogram through a texture for "tex" and "pairs".
+    bilinear fetch per sample, z interpolated in FP32) or "tma" (the same
+    z-pairs streamed by the Tensor Memory Accelerator into shared memory per
+    ray tile and interpolated there with FP32 weights; a tunable share of the
+    tiles still uses the texture unit). The backprojector samples the
+    sinogram through a texture for "tex", "pairs" and "tma".
     ``stage_f16`` stages projected volumes as FP16 ("soft"/"tex").
     ``adjoint`` keeps a per-ray table that speeds up :meth:`adjoint`
     (32 bytes per ray and view)."""
 
     def __init__(self, geometry: Geometry, max_batch: int = 1, sampler: str = "soft",
                  stage_f16: bool = False, device=None, adjoint: bool = False):
-        if sampler not in ("soft", "tex", "pairs"):
-            raise ValueError("sampler must be 'soft', 'tex' or 'pairs'")
+        if sampler not in SAMPLERS:
+            raise ValueError(f"sampler must be one of {SAMPLERS}")
         dev = torch.device("cuda", torch.cuda.current_device()) if device is None else \
             torch.device(device)
         if dev.type != "cuda":
@@ -155,7 +161,8 @@ class Plan:
         self.max_batch = int(max_batch)
         self.sampler = sampler
         self.stage_f16 = bool(stage_f16)
-        flags = {"soft": 0, "tex": _lib.DTV_PLAN_TEX, "pairs": _lib.DTV_PLAN_TEX_PAIRS}[sampler] | \
+        flags = {"soft": 0, "tex": _lib.DTV_PLAN_TEX, "pairs": _lib.DTV_PLAN_TEX_PAIRS,
+                 "tma": _lib.DTV_PLAN_TEX_PAIRS | _lib.DTV_PLAN_TMA}[sampler] | \
             (_lib.DTV_PLAN_STAGE_F16 if stage_f16 else 0) | (_lib.DTV_PLAN_ADJOINT if adjoint else 0)
         h = ctypes.c_void_p()
         call("dtv_plan_create", ctypes.byref(geometry.struct), self.max_batch, flags,
@@ -172,12 +179,20 @@ class Plan:
     def set_tuning(self, key: int, value: int) -> None:
         """Set a launch parameter (DTV_TUNE_*); results do not depend on it.
         DTV_TUNE_FP_RAY_TILE (0..7): the forward projector's block and warp
-        ray tile, which decides how compact each warp's texture footprint is."""
+        ray tile, which decides how compact each warp's texture footprint is
+        ("soft", "tex", "pairs"). DTV_TUNE_FP_TEX_SHARE (0..8, "tma" plans):
+        eighths of the ray tiles sampled through the texture unit."""
         call("dtv_plan_set_tuning", self._h, int(key), int(value))
 
     def get_tuning(self, key: int) -> int:
         out = ctypes.c_int32()
         call("dtv_plan_get_tuning", self._h, int(key), ctypes.byref(out))
+        return out.value
+
+    def device_status(self, reset: bool = True) -> int:
+        """Device-side error bits of this plan's kernels (0: none); synchronises."""
+        out = ctypes.c_int32()
+        call("dtv_plan_device_status", self._h, ctypes.byref(out), int(bool(reset)))
         return out.value
 
     def fp_samples(self) -> float:

@@ -73,6 +73,14 @@ extern "C" {
  * dtv_backward_adjoint, which otherwise rebuilds each ray for every 16^3
  * brick it crosses. */
 #define DTV_PLAN_ADJOINT 0x8
+/* With DTV_PLAN_TEX_PAIRS: the forward projector stages the z pairs of the
+ * volume a second time as a linear array and streams 20x32x20-word boxes of
+ * it into shared memory with the Tensor Memory Accelerator, one box per
+ * 16x16-ray tile and chunk of 16 planes along the tile's dominant axis;
+ * samples are interpolated from shared memory with FP32 x/y/z weights (exact
+ * trilinear of the FP16 volume). DTV_TUNE_FP_TEX_SHARE sends a share of the
+ * tiles through the texture unit instead, so both pipes work at once. */
+#define DTV_PLAN_TMA 0x10
 
 /* ---- forward-projector epilogues ---------------------------------------- */
 #define DTV_EPI_STORE 0    /* out = FP(vol)                                        */
@@ -168,8 +176,17 @@ DTV_API int dtv_plan_destroy(dtv_plan* plan);
  *   5 (8x32, 8x4), 6 (64x4, 32x1), 7 (8x32, 4x8).
  * No counterpart in the reference (its kernels use one fixed launch shape). */
 #define DTV_TUNE_FP_RAY_TILE 1
+/*   DTV_TUNE_FP_TEX_SHARE: with DTV_PLAN_TMA, how many eighths of the ray
+ *   tiles sample through the texture unit (0..8; the rest go through shared
+ *   memory). No counterpart in the reference. */
+#define DTV_TUNE_FP_TEX_SHARE 2
 DTV_API int dtv_plan_set_tuning(dtv_plan* plan, int32_t key, int32_t value);
 DTV_API int dtv_plan_get_tuning(const dtv_plan* plan, int32_t key, int32_t* value);
+/* Device-side error bits of the plan's kernels (0: none; 1: a shared-memory
+ * staging wait of the DTV_PLAN_TMA forward projector ran out of its iteration
+ * limit, the outputs of that launch are invalid). Synchronises the device;
+ * reset != 0 clears the bits. No counterpart in the reference. */
+DTV_API int dtv_plan_device_status(dtv_plan* plan, int32_t* status, int32_t reset);
 /* Number of forward-projector ray samples per volume (exact chord count under
  * the plan's phase rule, the algorithmic work unit), computed on the host. */
 DTV_API int dtv_plan_fp_samples(const dtv_plan* plan, double* samples_per_volume);

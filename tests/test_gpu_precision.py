@@ -26,7 +26,7 @@ def reduced(cuda, n=48, views=12):
     return geo, og, truth
 
 
-@pytest.mark.parametrize("sampler", ["soft", "tex", "pairs"])
+@pytest.mark.parametrize("sampler", ["soft", "tex", "pairs", "tma"])
 def test_projection_gate(cuda, sampler):
     geo, og, truth = reduced(cuda)
     plan = dtvb200.Plan(geo, sampler=sampler, device=cuda)
@@ -40,7 +40,8 @@ def test_projection_gate(cuda, sampler):
 
 @pytest.mark.parametrize("sampler,fdt", [("soft", torch.float32), ("tex", torch.float32),
                                          ("pairs", torch.float32), ("tex", torch.float16),
-                                         ("pairs", torch.float16)])
+                                         ("pairs", torch.float16), ("tma", torch.float32),
+                                         ("tma", torch.float16)])
 def test_dtv_reconstruction_gate(cuda, sampler, fdt):
     geo, og, truth = reduced(cuda)
     sino = O.forward(og, truth).reshape(1, 1, *og.sino_shape)
@@ -76,7 +77,7 @@ def test_full_size_linearity_and_samplers(cuda, full):
     rhs = a * soft.forward(x) + b * soft.forward(y)
     assert float(((lhs - rhs).double() ** 2).mean().sqrt() / (rhs.double() ** 2).mean().sqrt()) < 1e-5
     ref = soft.forward(x).double()
-    for sampler in ("tex", "pairs"):
+    for sampler in ("tex", "pairs", "tma"):
         out = dtvb200.Plan(geo, sampler=sampler, device=cuda).forward(x).double()
         assert float(((out - ref) ** 2).mean().sqrt() / (ref ** 2).mean().sqrt()) < GATE
 

@@ -87,6 +87,52 @@ def test_forward_pairs_matches_oracle(cuda, kind):
     assert rel_rmse(out, O.forward(og, vol).reshape(out.shape)) < 1e-3
 
 
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("share", [0, 3])
+@pytest.mark.parametrize("batch", [1, 2])
+def test_forward_tma_matches_oracle(cuda, kind, share, batch):
+    """Shared-memory z-pair sampler: FP16 planes, FP16 x/y and FP32 z weights;
+    with a share of the tiles through the texture unit (1/256 x/y weights)."""
+    g, og = make_case(kind)
+    plan = dtvb200.Plan(g, max_batch=2, sampler="tma", device=cuda)
+    plan.set_tuning(_lib.DTV_TUNE_FP_TEX_SHARE, share)
+    vol = blob_volume(np.random.default_rng(23), og.vol_shape, batch)
+    v16 = vol.astype(np.float16).astype(np.float32)
+    out = plan.forward(to_dev(vol, cuda)).cpu().numpy()
+    assert plan.device_status() == 0
+    assert rel_rmse(out, O.forward(og, v16).reshape(out.shape)) < (1e-4 if share == 0 else 5e-4)
+    assert rel_rmse(out, O.forward(og, vol).reshape(out.shape)) < 1e-3
+
+
+def test_forward_tma_all_texture_equals_pairs(cuda):
+    g, og = make_case("standard_odd")
+    vol = to_dev(blob_volume(np.random.default_rng(24), og.vol_shape, 1), cuda)
+    tma = dtvb200.Plan(g, sampler="tma", device=cuda)
+    tma.set_tuning(_lib.DTV_TUNE_FP_TEX_SHARE, 8)
+    assert torch.equal(tma.forward(vol), dtvb200.Plan(g, sampler="pairs", device=cuda).forward(vol))
+    with pytest.raises(dtvb200.DtvError):
+        dtvb200.Plan(g, sampler="pairs", device=cuda).set_tuning(_lib.DTV_TUNE_FP_TEX_SHARE, 1)
+    with pytest.raises(dtvb200.DtvError):
+        tma.set_tuning(_lib.DTV_TUNE_FP_TEX_SHARE, 9)
+
+
+def test_forward_tma_full_size_views(cuda):
+    """Chunk schedules of a 128^3 volume on a 192^2 detector at every
+    orientation class (axis-aligned, 45 degrees, both chunk axes and
+    directions) against the soft sampler on the FP16-rounded volume."""
+    n, nd = 128, 192
+    ang = np.arange(0, 360, 7.5)
+    g = dtvb200.circular(ang, (n, n, n), (1.0,) * 3, (nd, nd), (1.2, 1.2), 500.0, 1000.0)
+    from dtvb200.phantom import ellipsoids
+    x = ellipsoids((n, n, n), seed=5, device=cuda).half().float()
+    ref = dtvb200.Plan(g, sampler="soft", device=cuda).forward(x).double()
+    tma = dtvb200.Plan(g, sampler="tma", device=cuda)
+    out = tma.forward(x).double()
+    assert tma.device_status() == 0
+    assert float(((out - ref) ** 2).mean().sqrt() / (ref ** 2).mean().sqrt()) < 1e-4
+    assert float((out - ref).abs().max() / ref.abs().max()) < 1e-3
+
+
 @pytest.mark.parametrize("sampler", ["soft", "tex", "pairs"])
 def test_forward_ray_tiles_agree(cuda, sampler):
     """Every ray tile computes the same per-ray sums (bit-identical), with
@@ -121,7 +167,7 @@ def test_tuning_keys_and_autotune(cuda):
 
 
 @pytest.mark.parametrize("kind", KINDS)
-@pytest.mark.parametrize("sampler", ["soft", "tex", "pairs"])
+@pytest.mark.parametrize("sampler", ["soft", "tex", "pairs", "tma"])
 def test_backward_fdk_matches_oracle(cuda, kind, sampler):
     g, og = make_case(kind)
     plan = dtvb200.Plan(g, max_batch=2, sampler=sampler, device=cuda)
@@ -185,9 +231,10 @@ def test_forward_stage_f16(cuda):
     assert rel_rmse(out, O.forward(og, vol).reshape(out.shape)) < 1e-3
 
 
-def test_forward_epilogues(cuda):
+@pytest.mark.parametrize("sampler", ["soft", "tma"])
+def test_forward_epilogues(cuda, sampler):
     g, og = make_case("standard_odd")
-    plan = dtvb200.Plan(g, device=cuda)
+    plan = dtvb200.Plan(g, sampler=sampler, device=cuda)
     rng = np.random.default_rng(17)
     vol = to_dev(blob_volume(rng, og.vol_shape, 1), cuda)
     gs = to_dev(rng.random((1, 1) + og.sino_shape), cuda)
@@ -203,12 +250,13 @@ def test_forward_epilogues(cuda):
     assert torch.allclose(w, (w0 + sigma * (fp - gs)) / (1 + sigma), atol=1e-6)
 
 
-def test_rays_missing_the_volume_give_zero(cuda):
+@pytest.mark.parametrize("sampler", ["soft", "tma"])
+def test_rays_missing_the_volume_give_zero(cuda, sampler):
     # detector shifted far off axis: no ray meets the volume
     ang = np.array([0.0, 90.0], dtype=np.float32)
     g = dtvb200.standard(ang, (8, 8, 4), (16, 16), 500.0, 1000.0)
     g.views[:, 5] += 5000.0  # move the detector centres up along z
-    plan = dtvb200.Plan(g, device=cuda)
+    plan = dtvb200.Plan(g, sampler=sampler, device=cuda)
     out = plan.forward(torch.ones(g.vol_shape(1), device=cuda))
     assert float(out.abs().max()) == 0.0
 
