@@ -365,16 +365,23 @@ def run_ours(args):
         s16 = time_steps(lambda: alg16.run(img, sino), args.steps, stream)
         f16 = alg16.run(img, sino)
         err16 = float(torch.sqrt(((f16 - ref_f).double() ** 2).mean() / (ref_f.double() ** 2).mean()))
-        plain = dtvb200.DTVCP(plan, c["iters"], t_refresh=10, use_graph=False, **prm)
-        plain.run(img, sino)
-        sp = time_steps(lambda: plain.run(img, sino), args.steps, stream)
         extra = {
             "fp16_storage": {"value": units * args.steps / s16 / 1e9,
                              "recon_per_s": args.steps / s16,
                              "rel_rmse_vs_fp32_storage": err16},
-            "plain_fp32_eager": {"value": units * args.steps / sp / 1e9,
-                                 "recon_per_s": args.steps / sp},
         }
+        # the plain FP32 single-volume path: FP32 staging and FP32 weights,
+        # one launch per operator, no graph ("soft"); and the same through an
+        # FP32 3-D texture, as the reference samples ("tex")
+        for name, smp in (("plain_fp32_eager", "soft"), ("plain_fp32_tex_eager", "tex")):
+            pplan = dtvb200.Plan(geo, max_batch=1, sampler=smp, device=dev)
+            plain = dtvb200.DTVCP(pplan, c["iters"], t_refresh=10, use_graph=False, **prm)
+            plain.run(img, sino)
+            sp = time_steps(lambda: plain.run(img, sino), args.steps, stream)
+            extra[name] = {"value": units * args.steps / sp / 1e9, "recon_per_s": args.steps / sp,
+                           "sampler": smp}
+            del plain, pplan
+        extra["speedup_vs_plain_fp32"] = recon_s / extra["plain_fp32_eager"]["recon_per_s"]
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -389,6 +396,8 @@ def run_ours(args):
         "config": {"workload": workload_name(c), "parallelism": f"replicas x{ws}",
                    "sampler": args.sampler, "graph": "one CUDA graph per reconstruction",
                    "l2": "working set > L2 (volume, 4 dual volumes, sinograms ~0.5 GB)",
+                   "storage": ("f, duals, sinograms FP32; the projected volume staged as "
+                               "FP16 z-pairs; FP32 accumulation"),
                    "inputs": "seeded ellipsoid phantom, Poisson noise"},
         "recon_per_s": recon_s,
         "samples_per_recon": units,
@@ -535,6 +544,142 @@ def run_train(args):
     return 0
 
 
+def run_fista64(args):
+    """Plain method, small: 64^3 ellipsoid phantom (1 mm voxels), 60 views over
+    360 deg on a 128x128 detector at 1.0 mm pitch, SOD 500 / SDD 1000. One step
+    = forward projection of the phantom, one backprojection, then 20 FISTA-TV
+    (FISTA with directional-TV thresholds) iterations, as one CUDA graph."""
+    import numpy as np
+    import torch
+
+    import dtvb200
+    from dtvb200.algorithms import power_norm
+    dev = torch.device("cuda", 0)
+    c = dict(CFG, nx=64, ny=64, nz=64, nu=128, nv=128, pitch=1.0, n_views=60, iters=20)
+    geo, truth, _ = make_problem(dev, c, c["seed"])
+    V = 64 ** 3
+
+    def build(sampler, graph):
+        plan = dtvb200.Plan(geo, max_batch=1, sampler=sampler, device=dev)
+        sigma = dtv_params(plan, dev)["sigma"]
+        v = tuple(power_norm((64, 64, 64), a, False, device=dev) for a in range(3))
+        alg = dtvb200.DTVFISTA(plan, c["iters"], sigma=sigma, v=v, t=(1e-3,) * 3, quirk=False)
+        out_s = torch.empty(plan.sino_shape(1), device=dev)
+        out_b = torch.empty(plan.vol_shape(1), device=dev)
+        img = torch.zeros(plan.vol_shape(1), device=dev)
+
+        def body():
+            plan.forward(truth, out=out_s)
+            plan.backward(out_s, out=out_b)
+            alg.run(img, out_s)
+        if not graph:
+            return plan, body
+        g = torch.cuda.CUDAGraph()
+        body()  # allocate state outside the capture
+        torch.cuda.synchronize()
+        with torch.cuda.graph(g):
+            body()
+        return plan, g.replay
+
+    plan, step = build(args.sampler, True)
+    units = (c["iters"] + 1) * (plan.fp_samples() + V * c["n_views"])
+    stream = torch.cuda.current_stream(dev)
+    L = dtvb200._lib.load()
+    for _ in range(max(args.warmup, 1)):
+        step()
+    n0 = L.dtv_launch_count()
+    step()
+    torch.cuda.synchronize()
+    launches = L.dtv_launch_count() - n0  # a replay counts none: count an eager pass
+    _, eager = build(args.sampler, False)
+    n0 = L.dtv_launch_count()
+    eager()
+    launches = L.dtv_launch_count() - n0
+    with ClockSampler(0) as clk:
+        secs = time_steps(step, args.steps, stream)
+    _, plain = build("soft", False)
+    plain()
+    ps = time_steps(plain, args.steps, stream)
+    line = {
+        "metric": METRIC, "value": units * args.steps / secs / 1e9, "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "64^3 x 1 mm, 60 views/360deg, 128x128 det @ 1.0 mm, SOD 500 "
+                               "SDD 1000: FP + BP + 20 FISTA-TV iterations",
+                   "sampler": args.sampler, "graph": "one CUDA graph per step"},
+        "recon_per_s": args.steps / secs,
+        "plain_fp32_eager": {"value": units * args.steps / ps / 1e9, "recon_per_s": args.steps / ps,
+                             "sampler": "soft"},
+        "gpu_launches": launches * args.steps,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_large512(args):
+    """Large: 512^3 ellipsoid phantom (1 mm voxels), 1024x768 detector at
+    0.8 mm pitch, SOD 500 / SDD 1000. One step = the 360-view full-scan forward
+    projection plus 50 DTV iterations from the 90-view sparse subset (every
+    4th view), FP32-stored and BF16-stored (the volume and fbar in BF16; FP32
+    iterates and accumulation)."""
+    import numpy as np
+    import torch
+
+    import dtvb200
+    from dtvb200.phantom import ellipsoids
+    dev = torch.device("cuda", 0)
+    n, nu, nv, pitch, views, sparse, iters = 512, 1024, 768, 0.8, 360, 90, 50
+    ang = np.linspace(0, 360, views, endpoint=False)
+    geo = dtvb200.circular(ang, (n, n, n), (1.0,) * 3, (nu, nv), (pitch, pitch), 500.0, 1000.0)
+    geo_s = dtvb200.circular(ang[::views // sparse], (n, n, n), (1.0,) * 3, (nu, nv),
+                             (pitch, pitch), 500.0, 1000.0)
+    truth = ellipsoids((n, n, n), seed=CFG["seed"], device=dev)
+    full = dtvb200.Plan(geo, max_batch=1, sampler=args.sampler, device=dev)
+    plan = dtvb200.Plan(geo_s, max_batch=1, sampler=args.sampler, device=dev)
+    prm = dtv_params(plan, dev, iters=4)
+    sino_full = torch.empty(full.sino_shape(1), device=dev)
+    V = n ** 3
+    units = full.fp_samples() + iters * (plan.fp_samples() + V * sparse)
+    stream = torch.cuda.current_stream(dev)
+    res = {}
+    for name, dt in (("fp32", torch.float32), ("bf16", torch.bfloat16)):
+        vol = truth.to(dt)
+        alg = dtvb200.DTVCP(plan, iters, t_refresh=10, use_graph=True, f_dtype=dt, **prm)
+        img = torch.zeros(plan.vol_shape(1), device=dev)
+
+        def step():
+            full.forward(vol, out=sino_full)
+            return alg.run(img, sino_full[:, :, ::views // sparse].contiguous())
+        for _ in range(max(args.warmup, 1)):
+            f = step()
+        with ClockSampler(0) as clk:
+            secs = time_steps(step, args.steps, stream)
+        res[name] = {"secs": secs, "clocks": clk.summary(), "f": step(),
+                     "launches": alg.launches_per_run + 2}
+    err = float(torch.sqrt(((res["bf16"]["f"] - res["fp32"]["f"]).double() ** 2).mean()
+                           / (res["fp32"]["f"].double() ** 2).mean()))
+    secs = res["fp32"]["secs"]
+    line = {
+        "metric": METRIC, "value": units * args.steps / secs / 1e9, "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "512^3 x 1 mm, 1024x768 det @ 0.8 mm, SOD 500 SDD 1000: 360-view "
+                               "full-scan FP + 50 DTV iterations on the 90-view subset",
+                   "sampler": args.sampler, "graph": "one CUDA graph per reconstruction"},
+        "recon_per_s": args.steps / secs,
+        "bf16_storage": {"value": units * args.steps / res["bf16"]["secs"] / 1e9,
+                         "recon_per_s": args.steps / res["bf16"]["secs"],
+                         "rel_rmse_vs_fp32_storage": err},
+        "gpu_launches": res["fp32"]["launches"] * args.steps,
+        "clocks": res["fp32"]["clocks"],
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_profile(args):
     """N eager iterations of the workload (for ncu): forward projector,
     backprojector and fused updates, one launch each per iteration."""
@@ -565,15 +710,18 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--sampler", choices=["soft", "tex", "pairs"], default="pairs")
+    ap.add_argument("--sampler", choices=["soft", "tex", "pairs", "tma"], default="pairs")
     ap.add_argument("--small", action="store_true", help="64^3 smoke-size workload")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", choices=["sparse_dtv", "batch16", "train"],
+    ap.add_argument("--workload", choices=["sparse_dtv", "batch16", "train", "fista64",
+                                           "large512"],
                     default="sparse_dtv",
                     help="sparse_dtv: the headline workload; batch16: 16 heterogeneous FISTA "
                          "reconstructions batched into one graph; train: training steps of a "
-                         "10-stage unrolled network through the exact adjoint")
+                         "10-stage unrolled network through the exact adjoint; fista64: 64^3 "
+                         "FP + BP + 20 FISTA-TV iterations; large512: 512^3 360-view scan + "
+                         "50 DTV iterations on 90 views, FP32 and BF16 storage")
     ap.add_argument("--profile", type=int, default=0, metavar="N",
                     help="profiling run: N eager DTV iterations of the workload, no timing")
     args = ap.parse_args()
@@ -587,6 +735,10 @@ def main():
         return run_batch16(args)
     if args.workload == "train":
         return run_train(args)
+    if args.workload == "fista64":
+        return run_fista64(args)
+    if args.workload == "large512":
+        return run_large512(args)
     return run_ours(args)
 
 

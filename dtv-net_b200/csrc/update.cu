@@ -17,6 +17,7 @@
 // a level shares one exponent, so its sum is kept exactly as an integer sum of
 // 24-bit significands. After the last level the bin is a single value and
 // lambda follows in closed form from the counts and sums above it.
+#include <atomic>
 #include <math.h>
 
 #include <algorithm>
@@ -826,7 +827,8 @@ int dtv_pdhg_dual(const void* fbar, float* p, float* q, float* s, float* c, cons
                   int32_t batch, const dtv_pdhg_params* prm, const double* t, void* ws,
                   void* stream) {
   DTV_CHECK(fbar && p && q && s && c && size && prm && t && ws, "NULL argument");
-  DTV_CHECK(prm->f_dtype == DTV_F32 || prm->f_dtype == DTV_F16, "f_dtype must be f32 or f16");
+  DTV_CHECK(prm->f_dtype == DTV_F32 || prm->f_dtype == DTV_F16 || prm->f_dtype == DTV_BF16,
+            "f_dtype must be f32, f16 or bf16");
   int rc = check_dims(size, batch);
   if (rc) return rc;
   Dims d = make_dims(size, prm->quirk);
@@ -843,18 +845,26 @@ int dtv_pdhg_dual(const void* fbar, float* p, float* q, float* s, float* c, cons
     pdhg_dual_kernel<float><<<grid3(d, batch), kBlock3, 0, st>>>(
         (const float*)fbar, p, q, s, c, d, prm->v[0] * sg, prm->v[1] * sg, prm->v[2] * sg,
         sg * prm->mu, ch); note_launch();
-  } else {
+  } else if (prm->f_dtype == DTV_F16) {
     pdhg_dual_kernel<__half><<<grid3(d, batch), kBlock3, 0, st>>>(
         (const __half*)fbar, p, q, s, c, d, prm->v[0] * sg, prm->v[1] * sg, prm->v[2] * sg,
         sg * prm->mu, ch); note_launch();
+  } else {
+    pdhg_dual_kernel<__nv_bfloat16><<<grid3(d, batch), kBlock3, 0, st>>>(
+        (const __nv_bfloat16*)fbar, p, q, s, c, d, prm->v[0] * sg, prm->v[1] * sg,
+        prm->v[2] * sg, sg * prm->mu, ch); note_launch();
   }
   DTV_LAUNCH_CHECK();
-  static bool attr = false;
+  // the shared-memory limit is a per-device function attribute
+  static std::atomic<unsigned long long> attr_set{0};
   const int smem3 = 9 * kL1B3 * (int)sizeof(unsigned int);
-  if (!attr) {
+  int dev = 0;
+  DTV_CUDA_TRY(cudaGetDevice(&dev));
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (!(attr_set.load() & bit)) {
     DTV_CUDA_TRY(cudaFuncSetAttribute(l1_hist3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       smem3));
-    attr = true;
+    attr_set |= bit;
   }
   const int smem2 = 9 * kL1B2 * (int)sizeof(unsigned int);
   l1_select_kernel<<<3, 1024, 0, st>>>(ch, 1); note_launch();
@@ -871,7 +881,8 @@ int dtv_pdhg_primal(float* f, void* fbar, const float* recon, float* p, float* q
                     const float* c, const int32_t size[3], int32_t batch,
                     const dtv_pdhg_params* prm, const void* ws, void* stream) {
   DTV_CHECK(f && fbar && recon && p && q && s && c && size && prm && ws, "NULL argument");
-  DTV_CHECK(prm->f_dtype == DTV_F32 || prm->f_dtype == DTV_F16, "f_dtype must be f32 or f16");
+  DTV_CHECK(prm->f_dtype == DTV_F32 || prm->f_dtype == DTV_F16 || prm->f_dtype == DTV_BF16,
+            "f_dtype must be f32, f16 or bf16");
   int rc = check_dims(size, batch);
   if (rc) return rc;
   Dims d = make_dims(size, prm->quirk);
@@ -880,9 +891,13 @@ int dtv_pdhg_primal(float* f, void* fbar, const float* recon, float* p, float* q
     pdhg_primal_kernel<float><<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(
         f, (float*)fbar, recon, p, q, s, c, d, prm->tau, prm->mu, prm->v[0], prm->v[1],
         prm->v[2], ch); note_launch();
-  } else {
+  } else if (prm->f_dtype == DTV_F16) {
     pdhg_primal_kernel<__half><<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(
         f, (__half*)fbar, recon, p, q, s, c, d, prm->tau, prm->mu, prm->v[0], prm->v[1],
+        prm->v[2], ch); note_launch();
+  } else {
+    pdhg_primal_kernel<__nv_bfloat16><<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(
+        f, (__nv_bfloat16*)fbar, recon, p, q, s, c, d, prm->tau, prm->mu, prm->v[0], prm->v[1],
         prm->v[2], ch); note_launch();
   }
   DTV_LAUNCH_CHECK();

@@ -26,7 +26,7 @@ from . import _lib
 from ._lib import call
 from .geometry import Plan, _ptr, _stream, check_input
 
-_FDT = {torch.float32: _lib.DTV_F32, torch.float16: _lib.DTV_F16}
+_FDT = {torch.float32: _lib.DTV_F32, torch.float16: _lib.DTV_F16, torch.bfloat16: _lib.DTV_BF16}
 
 
 def power_norm(size, axis: int, quirk: bool = True, iters: int = 10, seed: int = 0,
@@ -131,9 +131,9 @@ class DTVCP(_Graphable):
     recon = BP(w) (:40); dual ascent + L1-ball projections + non-negativity dual
     in one fused pass plus an exact device-side threshold search (:41-47);
     primal step and over-relaxation in one fused pass (:48-54).
-    ``f_dtype`` torch.float16 stores fbar, the projector input, in FP16; the
-    iterate f and all arithmetic stay FP32 (rounding f itself each iteration
-    would drop updates below its FP16 resolution).
+    ``f_dtype`` torch.float16 / torch.bfloat16 stores fbar, the projector
+    input, in 16 bits; the iterate f and all arithmetic stay FP32 (rounding f
+    itself each iteration would drop updates below the 16-bit resolution).
     """
 
     def __init__(self, plan: Plan, cascades: int = 30, sigma: float = 1e-7, tau: float = 1e-7,
@@ -141,7 +141,7 @@ class DTVCP(_Graphable):
                  f_dtype=torch.float32, t_refresh: int = 10, use_graph: bool = False,
                  backprojector: str = "fdk"):
         if f_dtype not in _FDT:
-            raise ValueError("f_dtype must be torch.float32 or torch.float16")
+            raise ValueError("f_dtype must be torch.float32, torch.float16 or torch.bfloat16")
         if backprojector not in ("fdk", "adjoint"):
             raise ValueError("backprojector must be 'fdk' or 'adjoint'")
         self.plan = plan
@@ -229,7 +229,7 @@ class DTVCP(_Graphable):
 
     def _prepare(self, image, sino):
         check_input(image, "image", self.plan.vol_shape(image.shape[0]),
-                    dtypes=(torch.float32, torch.float16))
+                    dtypes=(torch.float32, torch.float16, torch.bfloat16))
         key = (tuple(image.shape), image.device.index)
         st = self.__dict__.setdefault("_state", {}).get(key)
         if st is None:

@@ -17,7 +17,8 @@ import numpy as np
 import torch
 
 from . import _lib
-from .geometry import Geometry, Plan
+from ._lib import call
+from .geometry import Geometry, Plan, _ptr, _stream, check_input
 
 
 class Projector:
@@ -155,8 +156,39 @@ def cos_weight(n_views: int, detector_size, sdd: float) -> torch.Tensor:
     return torch.from_numpy(np.broadcast_to(w, (1, 1, n_views, H, W)).copy())
 
 
+def fbp_filter(rows: torch.Tensor, sdd: float, rows_per_view: int, mid_i: float, mid_j: float,
+               adjoint: bool = False) -> torch.Tensor:
+    """Cosine weight and Ram-Lak ramp of the FBP layers in one kernel
+    (dtv_fbp_filter): rows of the last dimension (even width), the cosine row
+    index is (row number) mod rows_per_view."""
+    check_input(rows, "rows")
+    width = rows.shape[-1]
+    out = torch.empty_like(rows)
+    call("dtv_fbp_filter", _ptr(rows), _ptr(out), rows.numel() // width, int(rows_per_view),
+         int(width), float(sdd), float(mid_i), float(mid_j), int(bool(adjoint)),
+         _stream(rows.device))
+    return out
+
+
+class RampFilter(torch.autograd.Function):
+    """The FBP filter as a differentiable op; its gradient is the transpose
+    (ramp, then the cosine weight)."""
+
+    @staticmethod
+    def forward(ctx, rows, sdd, rows_per_view, mid_i, mid_j):
+        ctx.args = (sdd, rows_per_view, mid_i, mid_j)
+        return fbp_filter(rows.contiguous(), sdd, rows_per_view, mid_i, mid_j)
+
+    @staticmethod
+    def backward(ctx, grad):
+        return (fbp_filter(grad.contiguous(), *ctx.args, adjoint=True), None, None, None, None)
+
+
 class StandardGeometryWithFBP(torch.nn.Module):
-    """lamb * BP(ramp * (cos * (FP(x) - p)))  (StandardGeometry.py:45-66)."""
+    """lamb * BP(ramp * (cos * (FP(x) - p)))  (StandardGeometry.py:45-66).
+    ``cosWeight`` and ``ramp`` are kept as the reference's frozen parameters
+    (same state_dict keys); the weighting and filtering run fused in
+    dtv_fbp_filter."""
 
     def __init__(self, projector: Projector, sdd: float, matched: bool = False):
         super().__init__()
@@ -166,14 +198,46 @@ class StandardGeometryWithFBP(torch.nn.Module):
         self.cosWeight = torch.nn.Parameter(cos_weight(g.n_views, g.detector_size, sdd),
                                             requires_grad=False)
         self.ramp = torch.nn.Parameter(ramp_kernel(g.detector_size[0]), requires_grad=False)
-        self.width = g.detector_size[0]
+        self.width, self.height = g.detector_size
+        self.sdd = float(sdd)
 
     def forward(self, x, p):
         residual = self.FP.apply(x) - p
-        residual = residual * self.cosWeight
-        b, c, a, h, w = residual.size()
-        residual = residual.view(b, c, a * h, w)
-        residual = torch.nn.functional.conv2d(residual, self.ramp, stride=1,
-                                              padding=(0, int(self.width / 2)))
-        residual = residual.view(b, c, a, h, w)
-        return self.lamb * self.BP.apply(residual.contiguous())
+        residual = RampFilter.apply(residual, self.sdd, self.height, self.height / 2,
+                                    self.width / 2)
+        return self.lamb * self.BP.apply(residual)
+
+
+class BeijingGeometryWithFBP(torch.nn.Module):
+    """x - lamb * BP(filtered residual)  (BeijingGeometry.py:50-72). As the
+    reference, the residual [1,1,A*planes,H,W] is reinterpreted as rows of
+    W*planes columns (A views of H rows), weighted with the reference's
+    midpoints (row offset from W*planes/2, column offset from H/2,
+    BeijingGeometry.py:66-72) and ramp-filtered along those rows."""
+
+    def __init__(self, projector: Projector, sdd: float, planes: int, matched: bool = False):
+        super().__init__()
+        g = projector.geometry
+        if g.n_views % planes:
+            raise ValueError("the view count must be a multiple of planes")
+        self.FP, self.BP = make_functions(projector, matched)
+        self.lamb = torch.nn.Parameter(torch.tensor(1.0), requires_grad=False)
+        self.width, self.height = g.detector_size
+        self.planes, self.angles = int(planes), g.n_views // planes
+        self.sdd = float(sdd)
+        row = self.width * self.planes
+        i = np.arange(self.height)[:, None] - row / 2
+        j = np.arange(row)[None, :] - self.height / 2
+        cw = (self.sdd / np.sqrt(self.sdd ** 2 + i ** 2 + j ** 2)).astype(np.float32)
+        self.cosWeight = torch.nn.Parameter(
+            torch.from_numpy(np.broadcast_to(cw, (1, 1, self.angles, self.height, row)).copy()),
+            requires_grad=False)
+        self.ramp = torch.nn.Parameter(ramp_kernel(row), requires_grad=False)
+
+    def forward(self, x, p):
+        residual = self.FP.apply(x) - p
+        shape = residual.shape
+        rows = residual.reshape(1, 1, self.angles, self.height, self.width * self.planes)
+        rows = RampFilter.apply(rows, self.sdd, self.height, self.width * self.planes / 2,
+                                self.height / 2)
+        return x - self.lamb * self.BP.apply(rows.reshape(shape))

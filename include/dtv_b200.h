@@ -191,6 +191,19 @@ DTV_API int dtv_plan_device_status(dtv_plan* plan, int32_t* status, int32_t rese
  * the plan's phase rule, the algorithmic work unit), computed on the host. */
 DTV_API int dtv_plan_fp_samples(const dtv_plan* plan, double* samples_per_volume);
 
+/* ---- FBP filter ------------------------------------------------------------ */
+/* Cosine weighting and spatial Ram-Lak ramp of the FBP layers
+ * (Standard/StandardGeometry.py:51-93, Beijing/BeijingGeometry.py:57-84), fused:
+ * out[r, u] = sum_t k[t] * cos(i, u + t - W/2) * in[r, u + t - W/2] over rows r of
+ * `width` (W) columns, zero outside the row, with the reference's W+1-tap kernel
+ * k (1/8 at the centre, -1/(2 pi^2 d^2) at odd offsets d, 0 at even ones) and
+ * cos(i, j) = sdd / sqrt(sdd^2 + (i - mid_i)^2 + (j - mid_j)^2), i = r mod
+ * rows_per_view. adjoint != 0 applies the transpose (ramp, then the weight).
+ * W even (the reference's reshape fails for odd W), at most 8192. */
+DTV_API int dtv_fbp_filter(const float* in, float* out, int64_t rows, int32_t rows_per_view,
+                           int32_t width, float sdd, float mid_i, float mid_j, int32_t adjoint,
+                           void* stream);
+
 /* ---- projectors ------------------------------------------------------------- */
 /* Ray-driven forward projector (Standard/plug/kernel/forwardKernel.cu:22-143;
  * Beijing/plug/kernel/forwardKernel.cu:17-135), one launch for all views and
@@ -281,7 +294,7 @@ typedef struct dtv_pdhg_params {
   float mu;     /* non-negativity weight (DTVCP.py:22)        */
   float v[3];   /* per-direction weights v1,v2,v3 (:19-21)   */
   int32_t quirk; /* reference D_y wrap (Gradients.py:18-25)   */
-  int32_t f_dtype; /* storage of fbar, the projector input: DTV_F32 or DTV_F16
+  int32_t f_dtype; /* storage of fbar, the projector input: DTV_F32, DTV_F16 or DTV_BF16
                       (f itself is always FP32) */
 } dtv_pdhg_params;
 

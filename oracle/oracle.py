@@ -418,3 +418,44 @@ def asdpocs_run(fp, bp, image, sino, size, cascades, beta=0.00005, beta_red=0.99
         beta *= beta_red                                         # :46
         f0 = f
     return np.maximum(f, 0)                                      # :47
+
+
+# ----------------------------------------------------------------- FBP filter
+def ramp_taps(width: int) -> np.ndarray:
+    """The W+1-tap spatial Ram-Lak kernel, float32 as the reference stores it
+    (Standard/StandardGeometry.py:83-93, Beijing/BeijingGeometry.py:74-84)."""
+    f = np.ones(width + 1, dtype=np.float32)
+    mid = np.floor(width / 2)
+    for i in range(width + 1):
+        if (i - mid) % 2 == 0:
+            f[i] = 0
+        else:
+            f[i] = -0.5 / (np.pi * np.pi * (i - mid) * (i - mid))
+        if i == mid:
+            f[i] = 1 / 8
+    return f
+
+
+def fbp_filter(rows, rows_per_view, sdd, mid_i, mid_j, adjoint=False) -> np.ndarray:
+    """Cosine weight then ramp cross-correlation of each row (padding W/2 on
+    both sides), in FP64 (StandardGeometry.py:51-65 and :68-74; the Beijing
+    layer passes its own midpoints, BeijingGeometry.py:57-72). rows: [..., W];
+    the cosine row index is (row number) mod rows_per_view. adjoint applies
+    the transpose: ramp first, weight after."""
+    x = np.asarray(rows, dtype=np.float64)
+    W = x.shape[-1]
+    x2 = x.reshape(-1, W)
+    i = (np.arange(x2.shape[0]) % rows_per_view)[:, None] - mid_i
+    j = np.arange(W)[None, :] - mid_j
+    cw = sdd / np.sqrt(sdd ** 2 + i ** 2 + j ** 2)
+    k = ramp_taps(W).astype(np.float64)
+    half = W // 2
+    src = x2 if adjoint else x2 * cw
+    pad = np.zeros((x2.shape[0], W + 2 * half))
+    pad[:, half:half + W] = src
+    out = np.zeros_like(x2)
+    for t in range(W + 1):
+        out += k[t] * pad[:, t:t + W]
+    if adjoint:
+        out *= cw
+    return out.reshape(x.shape)

@@ -162,3 +162,27 @@ def test_loops_pinned_to_reference():
     f = O.asdpocs_run(fp, bp, img0, sino, M.LOOP_VS, int(p[5]), beta=p[0], beta_red=p[1],
                       ng=int(p[2]), alpha=p[3], rmax=p[4])
     assert rel_max(f, z["asd_f"]) < 1e-5
+
+
+def test_fbp_filter_oracle_matches_reference_torch_lines():
+    """oracle.fbp_filter against the reference's own torch formulation
+    (cosine weight then conv2d with padding W/2, StandardGeometry.py:51-65) on
+    CPU in FP64, and its transpose by the dot test."""
+    import torch
+    rng = np.random.default_rng(0)
+    x = rng.random((2, 1, 3, 5, 16))
+    H, W, sdd = 5, 16, 1000.0
+    i = np.arange(H)[:, None] - H / 2
+    j = np.arange(W)[None, :] - W / 2
+    cw = sdd / np.sqrt(sdd ** 2 + i ** 2 + j ** 2)
+    k = torch.from_numpy(O.ramp_taps(W).astype(np.float64)).reshape(1, 1, 1, W + 1)
+    y = torch.nn.functional.conv2d(torch.from_numpy(x * cw).reshape(2, 1, 3 * H, W), k,
+                                   padding=(0, W // 2)).reshape(x.shape).numpy()
+    assert np.abs(y - O.fbp_filter(x, H, sdd, H / 2, W / 2)).max() < 1e-12
+    z = rng.random(x.shape)
+    lhs = np.sum(O.fbp_filter(x, H, sdd, H / 2, W / 2) * z)
+    rhs = np.sum(x * O.fbp_filter(z, H, sdd, H / 2, W / 2, adjoint=True))
+    assert abs(lhs - rhs) < 1e-12 * abs(lhs)
+    taps = O.ramp_taps(8)
+    assert taps[4] == np.float32(1 / 8) and taps[2] == 0 and taps[3] == np.float32(-0.5 / np.pi ** 2)
+
