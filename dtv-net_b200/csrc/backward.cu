@@ -25,6 +25,13 @@ struct BPParams {
 };
 
 constexpr int kBPTile = 16;  // columns per block edge
+// Views whose 3x4 maps travel in one launch's parameters: read through the
+// constant cache, they leave the L1/texture pipe to the sinogram fetches.
+constexpr int kBPParamViews = 640;
+struct BPMaps {
+  float m[kBPParamViews][12];
+};
+static_assert(sizeof(BPMaps) <= 31 * 1024, "kernel parameter space");
 constexpr int kZC = 8;       // voxels per thread along z
 constexpr int kBPThreads = kBPTile * kBPTile;
 
@@ -49,7 +56,8 @@ struct SoftBil {
 // computes u, 1/h and the weight once and each voxel costs one FMA for v, one
 // fetch and one FMA.
 template <bool kTex, bool kZAff>
-__global__ void __launch_bounds__(kBPThreads) bp_kernel(BPParams bp, const BPView* __restrict__ views,
+__global__ void __launch_bounds__(kBPThreads) bp_kernel(BPParams bp, const __grid_constant__ BPMaps maps,
+                                                        int n0, int n_chunk,
                                                         const float* __restrict__ spad,
                                                         cudaTextureObject_t tex,
                                                         float* __restrict__ out, int accumulate) {
@@ -64,12 +72,12 @@ __global__ void __launch_bounds__(kBPThreads) bp_kernel(BPParams bp, const BPVie
   const float fi = (float)i, fj = (float)j;
   const int pu = bp.nu + 2 * kPad;
   const float mu = (float)bp.nu, mv = (float)bp.nv;
-  for (int n = 0; n < bp.n_views; ++n) {
-    const BPView& w = views[n];
-    const float m0 = __ldg(&w.m[0]), m1 = __ldg(&w.m[1]), m2 = __ldg(&w.m[2]), m3 = __ldg(&w.m[3]);
-    const float m4 = __ldg(&w.m[4]), m5 = __ldg(&w.m[5]), m6 = __ldg(&w.m[6]), m7 = __ldg(&w.m[7]);
-    const float m8 = __ldg(&w.m[8]), m9 = __ldg(&w.m[9]), m10 = __ldg(&w.m[10]),
-                m11 = __ldg(&w.m[11]);
+  for (int jn = 0; jn < n_chunk; ++jn) {
+    const int n = n0 + jn;
+    const float* w = maps.m[jn];
+    const float m0 = w[0], m1 = w[1], m2 = w[2], m3 = w[3];
+    const float m4 = w[4], m5 = w[5], m6 = w[6], m7 = w[7];
+    const float m8 = w[8], m9 = w[9], m10 = w[10], m11 = w[11];
     const float bu = fmaf(m0, fi, fmaf(m1, fj, m3));
     const float bv = fmaf(m4, fi, fmaf(m5, fj, m7));
     const float bh = fmaf(m8, fi, fmaf(m9, fj, m11));
@@ -154,6 +162,7 @@ int backward_impl(Plan* p, const float* sino, int batch, float* out, int accumul
   const int tiles = ((gp.nx + kBPTile - 1) / kBPTile) * ((gp.ny + kBPTile - 1) / kBPTile);
   dim3 grid(tiles, (gp.nz + kZC - 1) / kZC);
   const int64_t per_item = (int64_t)gp.nu * gp.nv * gp.n_views;
+  BPMaps maps;
   for (int b = 0; b < batch; ++b) {
     if (tex) {
       cudaMemcpy3DParms cp;
@@ -164,28 +173,31 @@ int backward_impl(Plan* p, const float* sino, int batch, float* out, int accumul
       cp.extent = make_cudaExtent(gp.nu, gp.nv, gp.n_views);
       cp.kind = cudaMemcpyDeviceToDevice;
       DTV_CUDA_TRY(cudaMemcpy3DAsync(&cp, st));
-      float* ob = out + (int64_t)b * gp.nx * gp.ny * gp.nz;
-      if (p->bp_zaffine) {
-        bp_kernel<true, true><<<grid, kBPThreads, 0, st>>>(bp, p->d_bpv, nullptr, p->sino_tex[0],
-                                                           ob, accumulate); note_launch();
-      } else {
-        bp_kernel<true, false><<<grid, kBPThreads, 0, st>>>(bp, p->d_bpv, nullptr, p->sino_tex[0],
-                                                            ob, accumulate); note_launch();
-      }
     } else {
       stage_sino_pad_kernel<<<(int)std::min<int64_t>((per_item + 255) / 256, 148 * 16), 256, 0,
                               st>>>(sino + b * per_item, p->d_sino_pad, gp.nu, gp.nv, gp.n_views); note_launch();
       DTV_LAUNCH_CHECK();
-      float* ob = out + (int64_t)b * gp.nx * gp.ny * gp.nz;
-      if (p->bp_zaffine) {
-        bp_kernel<false, true><<<grid, kBPThreads, 0, st>>>(bp, p->d_bpv, p->d_sino_pad, 0, ob,
-                                                            accumulate); note_launch();
-      } else {
-        bp_kernel<false, false><<<grid, kBPThreads, 0, st>>>(bp, p->d_bpv, p->d_sino_pad, 0, ob,
-                                                             accumulate); note_launch();
-      }
     }
-    DTV_LAUNCH_CHECK();
+    float* ob = out + (int64_t)b * gp.nx * gp.ny * gp.nz;
+    const cudaTextureObject_t tx = tex ? p->sino_tex[0] : 0;
+    const float* sp = tex ? nullptr : p->d_sino_pad;
+    // views in chunks of kBPParamViews; later chunks accumulate
+    for (int n0 = 0; n0 < gp.n_views; n0 += kBPParamViews) {
+      const int cnt = std::min(kBPParamViews, gp.n_views - n0);
+      for (int j = 0; j < cnt; ++j) memcpy(maps.m[j], p->h_bpv[n0 + j].m, sizeof(maps.m[j]));
+      const int acc = n0 > 0 ? 1 : accumulate;
+      if (tex && p->bp_zaffine) {
+        bp_kernel<true, true><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, ob, acc);
+      } else if (tex) {
+        bp_kernel<true, false><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, ob, acc);
+      } else if (p->bp_zaffine) {
+        bp_kernel<false, true><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, ob, acc);
+      } else {
+        bp_kernel<false, false><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, ob, acc);
+      }
+      note_launch();
+      DTV_LAUNCH_CHECK();
+    }
   }
   return DTV_OK;
 }

@@ -108,6 +108,7 @@ struct Plan {
   GeomParams gp;
   FPView* d_fpv;  // device
   BPView* d_bpv;  // device
+  BPView* h_bpv;  // host copy (the backprojector passes the maps as launch parameters)
   // soft sampler staging: zero-padded volumes (border kPad) of max_batch items
   void* d_vol_pad;
   int stage_dtype;    // DTV_F32 or DTV_F16

@@ -124,8 +124,10 @@ __global__ void __launch_bounds__(kFPThreads) fp_pair_kernel(RayParams rp, const
 
 // Writes the z-pair layers of one volume: layer L = (f[L-2], f[L-1]), zero
 // outside [0, nz), to the layered texture and, when `lin` is set, to the
-// linear [nz+3][ny][pitch] copy. One thread per (x, y) column walks the
-// nz + 3 layers.
+// linear [nz+3][ny][pitch] copy. A thread owns one (x, y) column and a run of
+// kStageLayers layers (grid z), so the whole volume is in flight at once.
+constexpr int kStageLayers = 16;
+
 template <class Tin>
 __global__ void __launch_bounds__(256) stage_pairs_kernel(const Tin* __restrict__ in,
                                                           cudaSurfaceObject_t surf,
@@ -134,13 +136,18 @@ __global__ void __launch_bounds__(256) stage_pairs_kernel(const Tin* __restrict_
   const int x = blockIdx.x * 32 + (threadIdx.x & 31);
   const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
   if (x >= nx || y >= ny) return;
+  const int L0 = blockIdx.z * kStageLayers;
+  const int L1 = min(L0 + kStageLayers, nz + 3);
   const int64_t plane = (int64_t)nx * ny;
   const Tin* col = in + (int64_t)y * nx + x;
-  __half prev = __float2half_rn(0.f);  // f[L-2]
-  for (int L = 0; L < nz + 3; ++L) {
-    const int z = L - 1;  // the new member f[L-1]
-    const __half cur = (z >= 0 && z < nz) ? __float2half_rn(load_as_float(col, z * plane))
-                                          : __float2half_rn(0.f);
+  auto member = [&](int z) {
+    return (z >= 0 && z < nz) ? __float2half_rn(load_as_float(col, z * plane))
+                              : __float2half_rn(0.f);
+  };
+  __half prev = member(L0 - 2);  // f[L-2]
+#pragma unroll 4
+  for (int L = L0; L < L1; ++L) {
+    const __half cur = member(L - 1);  // the new member f[L-1]
     const unsigned int bits = (unsigned int)__half_as_ushort(prev) |
                               ((unsigned int)__half_as_ushort(cur) << 16);
     surf2DLayeredwrite(bits, surf, x * 4, y, L);
@@ -228,7 +235,7 @@ template <class Tin>
 static int stage_volume_pairs(Plan* p, const Tin* vol, int batch, cudaStream_t st) {
   const GeomParams& g = p->gp;
   const int64_t vox = (int64_t)g.nx * g.ny * g.nz;
-  dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8);
+  dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + 3 + kStageLayers - 1) / kStageLayers);
   for (int b = 0; b < batch; ++b) {
     unsigned int* lin =
         p->d_pair_lin ? p->d_pair_lin + (int64_t)b * p->pair_pitch * g.ny * (g.nz + 3) : nullptr;

@@ -57,6 +57,7 @@ void free_plan(Plan* p) {
   cudaFree(p->d_status);
   cudaFree(p->d_fpv);
   cudaFree(p->d_bpv);
+  free(p->h_bpv);
   cudaFree(p->d_vol_pad);
   cudaFree(p->d_sino_pad);
   delete p;
@@ -131,6 +132,12 @@ int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Pla
   PLAN_CUDA(cudaMalloc(&p->d_bpv, sizeof(BPView) * gp.n_views));
   PLAN_CUDA(cudaMemcpy(p->d_fpv, fpv.data(), sizeof(FPView) * gp.n_views, cudaMemcpyHostToDevice));
   PLAN_CUDA(cudaMemcpy(p->d_bpv, bpv.data(), sizeof(BPView) * gp.n_views, cudaMemcpyHostToDevice));
+  p->h_bpv = (BPView*)malloc(sizeof(BPView) * gp.n_views);
+  if (!p->h_bpv) {
+    free_plan(p);
+    return fail(DTV_ERR_ALLOC, "host allocation failed");
+  }
+  memcpy(p->h_bpv, bpv.data(), sizeof(BPView) * gp.n_views);
 
   p->stage_dtype = (flags & DTV_PLAN_STAGE_F16) ? DTV_F16 : DTV_F32;
   p->pad_elems = (int64_t)(gp.nx + 2 * kPad) * (gp.ny + 2 * kPad) * (gp.nz + 2 * kPad);

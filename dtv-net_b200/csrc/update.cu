@@ -536,7 +536,21 @@ __global__ void __launch_bounds__(256) pdhg_dual_kernel(const T* __restrict__ fb
   const int64_t i0 = ((int64_t)cl.z0 * d.Y + cl.y) * d.X + cl.x;
   const bool xv = cl.x < d.X - 1;
   const bool yv_clean = cl.y < d.Y - 1;
-  // phase 1: all slices' loads, stencils and stores (independent across k)
+  // phase 1: the duals of all slices are loaded first (a later slice's loads
+  // cannot move above an earlier slice's stores to the same arrays), then
+  // stencils and stores
+  float pv[kZS], qv[kZS], sv[kZS], cv[kZS];
+#pragma unroll
+  for (int k = 0; k < kZS; ++k) {
+    pv[k] = qv[k] = sv[k] = cv[k] = 0.f;
+    if (cl.in && k < cl.nz) {
+      const int64_t t = cl.base + i0 + k * plane;
+      pv[k] = p[t];
+      qv[k] = q[t];
+      sv[k] = s[t];
+      cv[k] = c[t];
+    }
+  }
   unsigned int keys[3][kZS];
 #pragma unroll
   for (int k = 0; k < kZS; ++k) {
@@ -550,11 +564,11 @@ __global__ void __launch_bounds__(256) pdhg_dual_kernel(const T* __restrict__ fb
       const float gy = yv ? load_as_float(fb, i + oy) - fc : -fc;
       const float gz = z < d.Z - 1 ? load_as_float(fb, i + plane) - fc : -fc;
       const int64_t t = cl.base + i;
-      const float np = fmaf(a0, gx, p[t]), nq = fmaf(a1, gy, q[t]), ns = fmaf(a2, gz, s[t]);
+      const float np = fmaf(a0, gx, pv[k]), nq = fmaf(a1, gy, qv[k]), ns = fmaf(a2, gz, sv[k]);
       p[t] = np;
       q[t] = nq;
       s[t] = ns;
-      c[t] = fminf(fmaf(smu, fc, c[t]), 0.f);  // -relu(-c - sigma*mu*fbar)
+      c[t] = fminf(fmaf(smu, fc, cv[k]), 0.f);  // -relu(-c - sigma*mu*fbar)
       keys[0][k] = __float_as_uint(np) & 0x7FFFFFFFu;
       keys[1][k] = __float_as_uint(nq) & 0x7FFFFFFFu;
       keys[2][k] = __float_as_uint(ns) & 0x7FFFFFFFu;
