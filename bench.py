@@ -34,10 +34,16 @@ UNIT = "GRay·samples/s"
 CFG = dict(nx=256, ny=256, nz=256, voxel=1.0, nu=384, nv=384, pitch=1.2, n_views=64,
            sod=500.0, sdd=1000.0, iters=100, i0=1e5, seed=2024)
 
+# Bilinear fetches per second of one B200's texture units for a 32-bit texel
+# (dtv-net_b200/probes/texture_fetch_rate.cu: 3.84 fetches per clock per SM at
+# 1965 MHz). The projectors issue one such fetch per forward-projector sample
+# and per backprojected voxel-view.
+TEXTURE_FETCH_PEAK = 1.116e12
+
 # DRAM traffic of one forward-projector launch on this workload
 # (dram__bytes_read.sum + dram__bytes_write.sum, one ncu --set full capture of
 # `python bench.py --profile 12`) and that capture's texture-pipe utilisation.
-FP_NCU = {"pairs": {"traffic": 274.856448e6 + 61.563648e6, "tex_pipe_pct": 94.2}}
+FP_NCU = {"pairs": {"traffic": 275.710976e6 + 61.128192e6, "tex_pipe_pct": 93.7}}
 
 
 def workload_name(c):
@@ -408,7 +414,14 @@ def run_ours(args):
                      "texture_pipe_pct_of_peak": FP_NCU.get(args.sampler, {}).get("tex_pipe_pct"),
                      "kernel": "forward projector (staging + ray kernel)",
                      "algorithmic_bytes_per_launch": fp_bytes,
-                     "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
+                     "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                     "texture": {
+                         "unit": "bilinear fetches/s",
+                         "peak": TEXTURE_FETCH_PEAK,
+                         "forward_achieved": fp_samples / (t_fp * 1e-3),
+                         "forward_frac": fp_samples / (t_fp * 1e-3) / TEXTURE_FETCH_PEAK,
+                         "backward_achieved": V * n_views / (t_bp * 1e-3),
+                         "backward_frac": V * n_views / (t_bp * 1e-3) / TEXTURE_FETCH_PEAK}},
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": P * 4,
