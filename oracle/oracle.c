@@ -405,12 +405,13 @@ static void ray_samples(const og_geometry* g, const double* S, const double* r, 
 void oracle_forward(const og_geometry* g, const double* views, const double* vol, int batch, int q,
                     double* sino) {
   const int nx = g->nx, ny = g->ny, nz = g->nz, nu = g->nu, nv = g->nv;
-#pragma omp parallel for collapse(2) schedule(dynamic)
+  /* one task per detector row, so that a few views still use every core */
+#pragma omp parallel for collapse(3) schedule(dynamic)
   for (int b = 0; b < batch; ++b)
-    for (int n = 0; n < g->n_views; ++n) {
-      const double* V = vol + (int64_t)b * nx * ny * nz;
-      const double* vw = views + 12 * n;
-      for (int v = 0; v < nv; ++v)
+    for (int n = 0; n < g->n_views; ++n)
+      for (int v = 0; v < nv; ++v) {
+        const double* V = vol + (int64_t)b * nx * ny * nz;
+        const double* vw = views + 12 * n;
         for (int u = 0; u < nu; ++u) {
           double S[3], r[3], a0;
           long nk;
