@@ -476,6 +476,14 @@ def run_batch16(args):
     with ClockSampler(0) as clk:
         secs = time_steps(lambda: batch.run(imgs, sinos), args.steps, stream)
 
+    # lockstep: one forward and one backprojector launch per iteration for all 16
+    lock = None
+    if args.sampler in ("pairs", "tma"):
+        lock = dtvb200.BatchedFISTA([a.plan for a in algs], 30, lamb=0.05, L=1e-3,
+                                    use_graph=True)
+        lock.run(imgs, sinos)
+        ls = time_steps(lambda: lock.run(imgs, sinos), args.steps, stream)
+
     def plain_all():
         for a, i, s in zip(plains, imgs, sinos):
             a.run(i, s)
@@ -494,6 +502,9 @@ def run_batch16(args):
         "plain_fp32_sequential_eager": {"value": units * args.steps / ps / 1e9,
                                         "recon_per_s": 16 * args.steps / ps, "sampler": "soft"},
         "speedup_vs_plain_fp32": ps / secs,
+        "lockstep_one_launch_per_operator": None if lock is None else {
+            "value": units * args.steps / ls / 1e9, "recon_per_s": 16 * args.steps / ls,
+            "gpu_launches_per_run": lock.launches_per_run},
         "gpu_launches": batch.launches_per_run * args.steps,
         "clocks": clk.summary(),
     }

@@ -55,16 +55,28 @@ struct SoftBil {
 // rotation axis, as in the circular orbits), so per column and view the kernel
 // computes u, 1/h and the weight once and each voxel costs one FMA for v, one
 // fetch and one FMA.
-template <bool kTex, bool kZAff>
-__global__ void __launch_bounds__(kBPThreads) bp_kernel(BPParams bp, const __grid_constant__ BPMaps maps,
-                                                        int n0, int n_chunk,
-                                                        const float* __restrict__ spad,
-                                                        cudaTextureObject_t tex,
-                                                        float* __restrict__ out, int accumulate) {
+// Where a view's 3x4 map comes from: the launch parameters (one chunk of
+// views) or the plan's device table.
+struct ParamMaps {
+  const BPMaps* m;
+  __device__ __forceinline__ const float* row(int jn) const { return m->m[jn]; }
+};
+struct TableMaps {
+  const BPView* v;  // first view of the chunk
+  __device__ __forceinline__ const float* row(int jn) const { return v[jn].m; }
+};
+
+// One block's columns: tile `tile` of 16x16 (x, y) columns, z-chunk `zc` of kZC
+// voxels, views n0 .. n0 + n_chunk - 1.
+template <bool kTex, bool kZAff, class Maps>
+__device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps, int n0, int n_chunk,
+                                           const float* __restrict__ spad, cudaTextureObject_t tex,
+                                           float* __restrict__ out, int accumulate, int tile,
+                                           int zc) {
   const int tiles_x = (bp.nx + kBPTile - 1) / kBPTile;
-  const int i = (blockIdx.x % tiles_x) * kBPTile + (threadIdx.x & 15);
-  const int j = (blockIdx.x / tiles_x) * kBPTile + (threadIdx.x >> 4);
-  const int k0 = blockIdx.y * kZC;
+  const int i = (tile % tiles_x) * kBPTile + (threadIdx.x & 15);
+  const int j = (tile / tiles_x) * kBPTile + (threadIdx.x >> 4);
+  const int k0 = zc * kZC;
   if (i >= bp.nx || j >= bp.ny) return;
   float acc[kZC];
 #pragma unroll
@@ -74,7 +86,7 @@ __global__ void __launch_bounds__(kBPThreads) bp_kernel(BPParams bp, const __gri
   const float mu = (float)bp.nu, mv = (float)bp.nv;
   for (int jn = 0; jn < n_chunk; ++jn) {
     const int n = n0 + jn;
-    const float* w = maps.m[jn];
+    const float* w = maps.row(jn);
     const float m0 = w[0], m1 = w[1], m2 = w[2], m3 = w[3];
     const float m4 = w[4], m5 = w[5], m6 = w[6], m7 = w[7];
     const float m8 = w[8], m9 = w[9], m10 = w[10], m11 = w[11];
@@ -132,6 +144,16 @@ __global__ void __launch_bounds__(kBPThreads) bp_kernel(BPParams bp, const __gri
       else o[k * plane] = acc[z];
     }
   }
+}
+
+template <bool kTex, bool kZAff>
+__global__ void __launch_bounds__(kBPThreads) bp_kernel(BPParams bp, const __grid_constant__ BPMaps maps,
+                                                        int n0, int n_chunk,
+                                                        const float* __restrict__ spad,
+                                                        cudaTextureObject_t tex,
+                                                        float* __restrict__ out, int accumulate) {
+  bp_columns<kTex, kZAff>(bp, ParamMaps{&maps}, n0, n_chunk, spad, tex, out, accumulate,
+                          (int)blockIdx.x, (int)blockIdx.y);
 }
 
 __global__ void stage_sino_pad_kernel(const float* __restrict__ in, float* __restrict__ out, int nu,
@@ -198,6 +220,81 @@ int backward_impl(Plan* p, const float* sino, int batch, float* out, int accumul
       note_launch();
       DTV_LAUNCH_CHECK();
     }
+  }
+  return DTV_OK;
+}
+
+// ---- several plans' backprojections in one launch ---------------------------------------
+// A flat grid over every plan's (column tile, z-chunk) blocks; a block finds
+// its plan by the blocks' prefix offsets (kernel parameters, read uniformly).
+// The maps come from each plan's device table. Texture plans only; each item's
+// sinogram is first copied into its plan's layered array.
+struct BPManyItem {
+  BPParams bp;
+  const BPView* views;
+  cudaTextureObject_t tex;
+  float* out;
+  int tiles;
+  int block0;
+  int zaffine;
+};
+struct BPMany {
+  BPManyItem it[kManyItems];
+  int count;
+};
+static_assert(sizeof(BPMany) <= 31 * 1024, "kernel parameter space");
+
+__global__ void __launch_bounds__(kBPThreads) bp_many_kernel(const __grid_constant__ BPMany m,
+                                                             int accumulate) {
+  int k = 0;
+  while (k + 1 < m.count && (int)blockIdx.x >= m.it[k + 1].block0) ++k;
+  const BPManyItem& it = m.it[k];
+  const int local = (int)blockIdx.x - it.block0;
+  const int tile = local % it.tiles, zc = local / it.tiles;
+  if (it.zaffine)
+    bp_columns<true, true>(it.bp, TableMaps{it.views}, 0, it.bp.n_views, nullptr, it.tex, it.out,
+                           accumulate, tile, zc);
+  else
+    bp_columns<true, false>(it.bp, TableMaps{it.views}, 0, it.bp.n_views, nullptr, it.tex, it.out,
+                            accumulate, tile, zc);
+}
+
+int backward_many_impl(Plan* const* plans, const float* const* sinos, float* const* outs, int count,
+                       int accumulate, cudaStream_t st) {
+  BPMany m;
+  for (int c0 = 0; c0 < count; c0 += kManyItems) {
+    const int cnt = std::min(kManyItems, count - c0);
+    int64_t blocks = 0;
+    for (int k = 0; k < cnt; ++k) {
+      Plan* p = plans[c0 + k];
+      const GeomParams& gp = p->gp;
+      cudaMemcpy3DParms cp;
+      memset(&cp, 0, sizeof(cp));
+      cp.srcPtr = make_cudaPitchedPtr((void*)sinos[c0 + k], gp.nu * sizeof(float), gp.nu, gp.nv);
+      cp.dstArray = p->sino_arrays[0];
+      cp.extent = make_cudaExtent(gp.nu, gp.nv, gp.n_views);
+      cp.kind = cudaMemcpyDeviceToDevice;
+      DTV_CUDA_TRY(cudaMemcpy3DAsync(&cp, st));
+      BPManyItem& it = m.it[k];
+      it.bp.nx = gp.nx; it.bp.ny = gp.ny; it.bp.nz = gp.nz;
+      it.bp.nu = gp.nu; it.bp.nv = gp.nv; it.bp.n_views = gp.n_views;
+      it.bp.power = gp.bp_power;
+      it.bp.extent = gp.bp_extent;
+      it.bp.scale = (float)gp.bp_scale;
+      it.bp.sino_pad_elems = 0;
+      it.views = p->d_bpv;
+      it.tex = p->sino_tex[0];
+      it.out = outs[c0 + k];
+      it.tiles = ((gp.nx + kBPTile - 1) / kBPTile) * ((gp.ny + kBPTile - 1) / kBPTile);
+      it.block0 = (int)blocks;
+      it.zaffine = p->bp_zaffine;
+      blocks += (int64_t)it.tiles * ((gp.nz + kZC - 1) / kZC);
+    }
+    DTV_CHECK(blocks < 2147483647LL, "too many blocks for one launch");
+    m.count = cnt;
+    bp_many_kernel<<<(unsigned)blocks, kBPThreads, 0, st>>>(m, accumulate);
+    note_launch();
+    DTV_LAUNCH_CHECK();
   }
   return DTV_OK;
 }

@@ -153,6 +153,13 @@ int backward_impl(Plan* p, const float* sino, int batch, float* out, int accumul
                   cudaStream_t st);
 int adjoint_impl(Plan* p, const float* sino, int batch, float* out, cudaStream_t st);
 int encode_pair_maps(Plan* p);
+// several plans' projections in one launch (forward.cu, backward.cu)
+constexpr int kManyItems = 24;  // plans per launch; more run in further launches
+int forward_many_impl(Plan* const* plans, const void* const* vols, int vol_dtype, float* const* outs,
+                      int count, int epilogue, const float* const* gs, float sigma,
+                      cudaStream_t st);
+int backward_many_impl(Plan* const* plans, const float* const* sinos, float* const* outs, int count,
+                       int accumulate, cudaStream_t st);
 int build_ray_table(Plan* p, cudaStream_t st);
 
 }  // namespace dtv

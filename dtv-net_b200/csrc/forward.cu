@@ -15,6 +15,7 @@
 //     software trilinear weights in FP32 (exact adjoint available), or through
 //     a texture object (hardware filtering, as the reference).
 #include <algorithm>
+#include <vector>
 #include <string.h>
 
 #include "ray.cuh"
@@ -291,6 +292,92 @@ int forward_impl(Plan* p, const void* vol, int vol_dtype, int batch, float* out,
                                                        p->pad_elems, o); note_launch();
   }
   DTV_LAUNCH_CHECK();
+  return DTV_OK;
+}
+
+// ---- several plans' forward projections in one launch -----------------------------------
+// A flat grid over every plan's (view, 16x16-ray tile) blocks, heaviest plans
+// first; a block finds its plan by the blocks' prefix offsets (kernel
+// parameters, read uniformly) and runs the z-pair sampler of fp_pair_kernel,
+// so each ray's sum is the same computation as a single-plan launch.
+struct FPManyItem {
+  RayParams rp;
+  const FPView* views;
+  cudaTextureObject_t tex;
+  FPOut o;
+  int tiles_u, tiles;
+  int block0;
+};
+struct FPMany {
+  FPManyItem it[kManyItems];
+  int count;
+};
+static_assert(sizeof(FPMany) <= 31 * 1024, "kernel parameter space");
+
+__global__ void __launch_bounds__(kFPThreads) fp_pair_many_kernel(const __grid_constant__ FPMany m) {
+  int k = 0;
+  while (k + 1 < m.count && (int)blockIdx.x >= m.it[k + 1].block0) ++k;
+  const FPManyItem& it = m.it[k];
+  const int local = (int)blockIdx.x - it.block0;
+  const int n = local / it.tiles, tile = local % it.tiles;
+  const int t = threadIdx.x, w = t >> 5, l = t & 31;
+  const int u = (tile % it.tiles_u) * 16 + (w & 1) * 8 + (l & 7);
+  const int v = (tile / it.tiles_u) * 16 + (w >> 1) * 4 + (l >> 3);
+  const RayParams& rp = it.rp;
+  if (u < rp.nu && v < rp.nv) {
+    const RaySetup rs = setup_ray(rp, it.views[n], u, v, 0.5f, 0.f);
+    PairSampler smp{it.tex, (float)(rp.nz + 2)};
+    const float val = rs.count > 0 ? ray_sum(smp, rs) * rp.scale : 0.f;
+    float res;
+    fp_store(rp, it.o, n, 0, u, v, val, res);
+  }
+}
+
+int forward_many_impl(Plan* const* plans, const void* const* vols, int vol_dtype, float* const* outs,
+                      int count, int epilogue, const float* const* gs, float sigma,
+                      cudaStream_t st) {
+  for (int k = 0; k < count; ++k) {
+    Plan* p = plans[k];
+    int rc;
+    switch (vol_dtype) {
+      case DTV_F32: rc = stage_volume_pairs(p, (const float*)vols[k], 1, st); break;
+      case DTV_F16: rc = stage_volume_pairs(p, (const __half*)vols[k], 1, st); break;
+      default: rc = stage_volume_pairs(p, (const __nv_bfloat16*)vols[k], 1, st); break;
+    }
+    if (rc) return rc;
+  }
+  // heaviest first (rays x volume edge), so the longest blocks start earliest
+  std::vector<int> order(count);
+  for (int k = 0; k < count; ++k) order[k] = k;
+  auto work = [&](int k) {
+    const GeomParams& g = plans[k]->gp;
+    return (double)g.n_views * g.nu * g.nv * std::max(g.nx, std::max(g.ny, g.nz));
+  };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
+  FPMany m;
+  for (int c0 = 0; c0 < count; c0 += kManyItems) {
+    const int cnt = std::min(kManyItems, count - c0);
+    int64_t blocks = 0;
+    for (int j = 0; j < cnt; ++j) {
+      const int k = order[c0 + j];
+      Plan* p = plans[k];
+      const GeomParams& gp = p->gp;
+      FPManyItem& it = m.it[j];
+      it.rp = make_ray_params(gp);
+      it.views = p->d_fpv;
+      it.tex = p->pair_tex[0];
+      it.o = FPOut{outs[k], gs ? gs[k] : nullptr, sigma, nullptr, epilogue};
+      it.tiles_u = (gp.nu + 15) / 16;
+      it.tiles = it.tiles_u * ((gp.nv + 15) / 16);
+      it.block0 = (int)blocks;
+      blocks += (int64_t)it.tiles * gp.n_views;
+    }
+    DTV_CHECK(blocks < 2147483647LL, "too many blocks for one launch");
+    m.count = cnt;
+    fp_pair_many_kernel<<<(unsigned)blocks, kFPThreads, 0, st>>>(m);
+    note_launch();
+    DTV_LAUNCH_CHECK();
+  }
   return DTV_OK;
 }
 

@@ -376,6 +376,43 @@ int dtv_backward(dtv_plan* plan, const float* sino, int32_t batch, float* out, i
   return backward_impl(p, sino, batch, out, accumulate, as_stream(stream));
 }
 
+int dtv_forward_many(dtv_plan* const* plans, const void* const* vols, int32_t vol_dtype,
+                     float* const* outs, int32_t count, int32_t epilogue, const float* const* gs,
+                     float sigma, void* stream) {
+  DTV_CHECK(plans && vols && outs, "NULL argument");
+  DTV_CHECK(count >= 1, "count %d < 1", count);
+  DTV_CHECK(dtype_ok(vol_dtype), "bad volume dtype %d", vol_dtype);
+  DTV_CHECK(epilogue >= DTV_EPI_STORE && epilogue <= DTV_EPI_PDHG, "bad epilogue %d", epilogue);
+  DTV_CHECK(epilogue == DTV_EPI_STORE || gs != nullptr, "epilogue %d needs g", epilogue);
+  std::vector<Plan*> ps(count);
+  for (int k = 0; k < count; ++k) {
+    DTV_CHECK(plans[k] && vols[k] && outs[k], "NULL plan, volume or output at %d", k);
+    DTV_CHECK(epilogue == DTV_EPI_STORE || gs[k], "NULL g at %d", k);
+    ps[k] = reinterpret_cast<Plan*>(plans[k]);
+    DTV_CHECK(ps[k]->flags & DTV_PLAN_TEX_PAIRS, "plan %d is not a DTV_PLAN_TEX_PAIRS plan", k);
+    DTV_CHECK(ps[k]->device == ps[0]->device, "plans %d and 0 are on different devices", k);
+  }
+  DeviceGuard dg(ps[0]->device);
+  return forward_many_impl(ps.data(), vols, vol_dtype, outs, count, epilogue, gs, sigma,
+                           as_stream(stream));
+}
+
+int dtv_backward_many(dtv_plan* const* plans, const float* const* sinos, float* const* outs,
+                      int32_t count, int32_t accumulate, void* stream) {
+  DTV_CHECK(plans && sinos && outs, "NULL argument");
+  DTV_CHECK(count >= 1, "count %d < 1", count);
+  std::vector<Plan*> ps(count);
+  for (int k = 0; k < count; ++k) {
+    DTV_CHECK(plans[k] && sinos[k] && outs[k], "NULL plan, sinogram or output at %d", k);
+    ps[k] = reinterpret_cast<Plan*>(plans[k]);
+    DTV_CHECK(ps[k]->sino_tex != nullptr,
+              "plan %d has no sinogram texture (DTV_PLAN_TEX or DTV_PLAN_TEX_PAIRS)", k);
+    DTV_CHECK(ps[k]->device == ps[0]->device, "plans %d and 0 are on different devices", k);
+  }
+  DeviceGuard dg(ps[0]->device);
+  return backward_many_impl(ps.data(), sinos, outs, count, accumulate ? 1 : 0, as_stream(stream));
+}
+
 int dtv_backward_adjoint(dtv_plan* plan, const float* sino, int32_t batch, float* out,
                          void* stream) {
   int rc = check_plan_call(plan, batch);

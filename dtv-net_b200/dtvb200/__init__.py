@@ -5,17 +5,18 @@ of include/dtv_b200.h; this package is its host side. There is no CPU path.
 """
 from . import _lib, autotune
 from ._lib import DtvError
-from .geometry import Geometry, Plan, circular, standard, vector
+from .geometry import Geometry, Plan, backward_many, circular, forward_many, standard, vector
 from .ops import (BeijingGeometry, BeijingGeometryWithFBP, Projector, RampFilter,
                   StandardGeometry, StandardGeometryWithFBP, fbp_filter, make_functions)
 from .tv import diff, diff_abs_sums, l1ball
-from .algorithms import ASDPOCS, DTVCP, DTVFISTA, FISTA, Batched, power_norm
+from .algorithms import ASDPOCS, DTVCP, DTVFISTA, FISTA, Batched, BatchedFISTA, power_norm
 
 __all__ = [
     "DtvError", "Geometry", "Plan", "circular", "standard", "vector", "Projector",
     "StandardGeometry", "StandardGeometryWithFBP", "BeijingGeometry", "BeijingGeometryWithFBP",
     "RampFilter", "fbp_filter", "make_functions", "diff",
-    "diff_abs_sums", "l1ball", "DTVCP", "FISTA", "DTVFISTA", "ASDPOCS", "Batched", "power_norm",
+    "diff_abs_sums", "l1ball", "DTVCP", "FISTA", "DTVFISTA", "ASDPOCS", "Batched", "BatchedFISTA",
+    "power_norm", "forward_many", "backward_many",
     "library_path",
 ]
 

@@ -267,3 +267,49 @@ class Plan:
             self.close()
         except Exception:
             pass
+
+
+def _ptr_array(ts):
+    return (ctypes.c_void_p * len(ts))(*[t.data_ptr() for t in ts])
+
+
+def forward_many(plans, vols, outs=None, epilogue: int = 0, gs=None, sigma: float = 0.0):
+    """Forward projections of several volumes, each with its own plan (any
+    sizes and view counts, "pairs" or "tma" plans on one device), in one
+    kernel launch (dtv_forward_many). Returns the list of sinograms."""
+    if not (len(plans) == len(vols) >= 1):
+        raise ValueError("need one volume per plan")
+    dt = vols[0].dtype
+    for p, v in zip(plans, vols):
+        check_input(v, "volume", p.vol_shape(1), dtypes=(dt,))
+    if outs is None:
+        outs = [torch.empty(p.sino_shape(1), device=v.device) for p, v in zip(plans, vols)]
+    for p, o in zip(plans, outs):
+        check_input(o, "out", p.sino_shape(1))
+    if gs is not None:
+        for p, g in zip(plans, gs):
+            check_input(g, "g", p.sino_shape(1))
+    call("dtv_forward_many", (ctypes.c_void_p * len(plans))(*[p._h.value for p in plans]),
+         _ptr_array(vols), _DT[dt], _ptr_array(outs), len(plans), int(epilogue),
+         _ptr_array(gs) if gs is not None else None, float(sigma), _stream(vols[0].device))
+    return outs
+
+
+def backward_many(plans, sinos, outs=None, accumulate: bool = False):
+    """FDK backprojections of several sinograms, each with its own plan
+    (texture-sampled plans on one device), in one kernel launch
+    (dtv_backward_many). Returns the list of volumes."""
+    if not (len(plans) == len(sinos) >= 1):
+        raise ValueError("need one sinogram per plan")
+    for p, s in zip(plans, sinos):
+        check_input(s, "sino", p.sino_shape(1))
+    if outs is None:
+        outs = [torch.empty(p.vol_shape(1), device=s.device) for p, s in zip(plans, sinos)]
+        accumulate = False
+    for p, o in zip(plans, outs):
+        check_input(o, "out", p.vol_shape(1))
+    call("dtv_backward_many", (ctypes.c_void_p * len(plans))(*[p._h.value for p in plans]),
+         _ptr_array(sinos), _ptr_array(outs), len(plans), int(bool(accumulate)),
+         _stream(sinos[0].device))
+    return outs
+
