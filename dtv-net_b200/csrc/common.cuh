@@ -140,6 +140,9 @@ struct Plan {
   int bp_zaffine;            // every view's u and h are independent of z
   // adjoint ray table (DTV_PLAN_ADJOINT): per view and pixel, (p0, count) and (dp, 0)
   float4* d_rays;
+  // adjoint cell records (DTV_PLAN_ADJOINT): (nx+1)(ny+1)nz float4 per batch item
+  float4* d_cells;
+  int adjoint_method;  // DTV_TUNE_ADJOINT
   double fp_samples;  // per volume, < 0 until computed
 };
 

@@ -53,6 +53,7 @@ void free_plan(Plan* p) {
   free(p->sino_arrays);
   cudaFree(p->vol_tex_dev);
   cudaFree(p->d_rays);
+  cudaFree(p->d_cells);
   cudaFree(p->d_pair_lin);
   cudaFree(p->d_status);
   cudaFree(p->d_fpv);
@@ -248,6 +249,9 @@ int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Pla
   if (flags & DTV_PLAN_ADJOINT) {
     const size_t n = (size_t)gp.n_views * gp.nu * gp.nv * 2;
     PLAN_CUDA(cudaMalloc(&p->d_rays, n * sizeof(float4)));
+    const size_t cells = (size_t)(gp.nx + 1) * (gp.ny + 1) * gp.nz * max_batch;
+    PLAN_CUDA(cudaMalloc(&p->d_cells, cells * sizeof(float4)));
+    p->adjoint_method = 1;
     rc = build_ray_table(p, 0);
     if (!rc) {
       cudaError_t e = cudaStreamSynchronize(0);
@@ -297,6 +301,11 @@ int dtv_plan_set_tuning(dtv_plan* plan, int32_t key, int32_t value) {
   DTV_CHECK(plan != nullptr, "plan is NULL");
   Plan* p = reinterpret_cast<Plan*>(plan);
   switch (key) {
+    case DTV_TUNE_ADJOINT:
+      DTV_CHECK(value == 0 || value == 1, "DTV_TUNE_ADJOINT must be 0 or 1");
+      DTV_CHECK(value == 0 || p->d_cells, "DTV_TUNE_ADJOINT 1 needs a DTV_PLAN_ADJOINT plan");
+      p->adjoint_method = value;
+      return DTV_OK;
     case DTV_TUNE_FP_TEX_SHARE:
       DTV_CHECK(p->flags & DTV_PLAN_TMA, "DTV_TUNE_FP_TEX_SHARE needs a DTV_PLAN_TMA plan");
       DTV_CHECK(value >= 0 && value <= 8, "DTV_TUNE_FP_TEX_SHARE must be in [0, 8]");
@@ -321,6 +330,9 @@ int dtv_plan_get_tuning(const dtv_plan* plan, int32_t key, int32_t* value) {
       return DTV_OK;
     case DTV_TUNE_FP_TEX_SHARE:
       *value = p->fp_tex_share;
+      return DTV_OK;
+    case DTV_TUNE_ADJOINT:
+      *value = p->adjoint_method;
       return DTV_OK;
     default:
       return fail(DTV_ERR_INVALID, "unknown tuning key %d", key);

@@ -69,9 +69,10 @@ extern "C" {
  * returns both planes and the z interpolation is done in FP32. Backprojector
  * as DTV_PLAN_TEX. Needs nz + 3 <= the device's layered-texture layer limit. */
 #define DTV_PLAN_TEX_PAIRS 0x4
-/* Keep a table of every ray's sample range (32 bytes per ray and view) for
+/* Keep a table of every ray's sample range (32 bytes per ray and view) and
+ * (nx+1)(ny+1)nz 16-byte cell records per batch item for
  * dtv_backward_adjoint, which otherwise rebuilds each ray for every 16^3
- * brick it crosses. */
+ * brick it crosses (see DTV_TUNE_ADJOINT). */
 #define DTV_PLAN_ADJOINT 0x8
 /* With DTV_PLAN_TEX_PAIRS: the forward projector stages the z pairs of the
  * volume a second time as a linear array and streams 20x32x20-word boxes of
@@ -180,6 +181,11 @@ DTV_API int dtv_plan_destroy(dtv_plan* plan);
  *   tiles sample through the texture unit (0..8; the rest go through shared
  *   memory). No counterpart in the reference. */
 #define DTV_TUNE_FP_TEX_SHARE 2
+/*   DTV_TUNE_ADJOINT: how dtv_backward_adjoint scatters, 0 = per 16^3 brick
+ *   through shared-memory atomics, 1 = into per-cell records of four floats
+ *   with 16-byte vector atomics, then a gather (needs DTV_PLAN_ADJOINT; the
+ *   default for such plans). No counterpart in the reference. */
+#define DTV_TUNE_ADJOINT 3
 DTV_API int dtv_plan_set_tuning(dtv_plan* plan, int32_t key, int32_t value);
 DTV_API int dtv_plan_get_tuning(const dtv_plan* plan, int32_t key, int32_t* value);
 /* Device-side error bits of the plan's kernels (0: none; 1: a shared-memory

@@ -7,6 +7,7 @@ import pytest
 import torch
 
 import dtvb200
+from dtvb200 import _lib
 import oracle as O
 from dtvb200.phantom import ellipsoids
 from helpers import rel_rmse
@@ -82,9 +83,12 @@ def test_full_size_linearity_and_samplers(cuda, full):
         assert float(((out - ref) ** 2).mean().sqrt() / (ref ** 2).mean().sqrt()) < GATE
 
 
-def test_full_size_adjoint_dot_test(cuda, full):
+@pytest.mark.parametrize("table,method", [(False, 0), (True, 1)])
+def test_full_size_adjoint_dot_test(cuda, full, table, method):
     geo, x = full
-    soft = dtvb200.Plan(geo, sampler="soft", device=cuda)
+    soft = dtvb200.Plan(geo, sampler="soft", device=cuda, adjoint=table)
+    if table:
+        soft.set_tuning(_lib.DTV_TUNE_ADJOINT, method)
     g = torch.Generator(device=cuda).manual_seed(3)
     y = torch.rand(soft.sino_shape(1), device=cuda, generator=g)
     lhs = float((soft.forward(x).double() * y.double()).sum())

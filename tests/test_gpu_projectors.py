@@ -194,10 +194,15 @@ def test_backward_accumulate(cuda):
 
 
 @pytest.mark.parametrize("kind", KINDS)
-@pytest.mark.parametrize("table", [False, True])
-def test_adjoint_matches_oracle_and_dot_test(cuda, kind, table):
+@pytest.mark.parametrize("table,method", [(False, 0), (True, 0), (True, 1)])
+def test_adjoint_matches_oracle_and_dot_test(cuda, kind, table, method):
+    """method 0: brick scatter through shared memory; 1: cell records with
+    vector atomics (needs the plan's adjoint tables)."""
     g, og = make_case(kind)
     plan = dtvb200.Plan(g, max_batch=2, device=cuda, adjoint=table)
+    if table:
+        plan.set_tuning(_lib.DTV_TUNE_ADJOINT, method)
+    assert plan.get_tuning(_lib.DTV_TUNE_ADJOINT) == method
     rng = np.random.default_rng(14)
     y = rng.random((2, 1) + og.sino_shape).astype(np.float32)
     x = rng.random((2, 1) + og.vol_shape).astype(np.float32)
@@ -345,6 +350,24 @@ def test_matches_reference_kernels_vector(cuda, sampler):
     tol = {"tex": 5e-4, "soft": 5e-3, "pairs": 2e-3}[sampler]
     assert rel_rmse(fp.cpu().numpy(), z["v_fp"]) < tol
     assert rel_rmse(bp.cpu().numpy(), z["v_bp"]) < tol
+
+
+@pytest.mark.parametrize("name", ["s1", "s2", "s3"])
+def test_reference_pairing_gradient_matches_reference_kernels(cuda, name):
+    """The reference's own gradient: its ForwardProjection.backward is the FDK
+    backprojection of the incoming gradient (StandardGeometry.py:17-21). The
+    gradient of FP through the reference pairing, with the golden sinogram as
+    the incoming gradient, equals what the reference kernels' backprojector
+    gave for that sinogram."""
+    z = _ref_proj()
+    X, Y, Z, W, H, n, b = (int(v) for v in z[f"{name}_sizes"])
+    sid, sdd = (float(v) for v in z[f"{name}_geom"])
+    geo = dtvb200.standard(z[f"{name}_angles"].astype(np.float32), (X, Y, Z), (W, H), sid, sdd)
+    FP, _ = dtvb200.make_functions(dtvb200.Projector(geo, sampler="tex", max_batch=b),
+                                   matched=False)
+    x = to_dev(z[f"{name}_vol"], cuda).requires_grad_()
+    FP.apply(x).backward(to_dev(z[f"{name}_sino_in"], cuda))
+    assert rel_rmse(x.grad.cpu().numpy(), z[f"{name}_bp"]) < 5e-4
 
 
 def test_standard_layers_autograd(cuda):
