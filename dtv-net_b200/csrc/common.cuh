@@ -111,6 +111,9 @@ struct Plan {
   BPView* h_bpv;  // host copy (the backprojector passes the maps as launch parameters)
   // soft sampler staging: zero-padded volumes (border kPad) of max_batch items
   void* d_vol_pad;
+  // FP32 soft plans: quad records (x..x+1, y..y+1 of one plane) over the same
+  // padded grid, read by the forward projector instead of d_vol_pad
+  float4* d_vol_quads;
   int stage_dtype;    // DTV_F32 or DTV_F16
   int64_t pad_elems;  // elements of one padded volume
   // soft bilinear staging: zero-padded sinogram of one batch item

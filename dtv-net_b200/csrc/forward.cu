@@ -46,6 +46,29 @@ struct SoftSampler {
   }
 };
 
+// The same trilinear interpolation from the quad copy of the padded volume:
+// record (x, y, z) = (f(x,y,z), f(x+1,y,z), f(x,y+1,z), f(x+1,y+1,z)), so a
+// sample makes two 16-byte loads (planes z and z+1) instead of eight 4-byte
+// ones, and the lerps run in the order of SoftSampler (same result bits).
+struct QuadSampler {
+  const float4* q;  // quad records of this batch item (padded indexing)
+  int px, pxy;
+  float mx, my, mz;
+  __device__ __forceinline__ float operator()(float x, float y, float z) const {
+    const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
+    const float ax = x - fx, ay = y - fy, az = z - fz;
+    const int ix = (int)fminf(fmaxf(fx, -2.f), mx) + kPad;
+    const int iy = (int)fminf(fmaxf(fy, -2.f), my) + kPad;
+    const int iz = (int)fminf(fmaxf(fz, -2.f), mz) + kPad;
+    const float4* b = q + (iz * pxy + iy * px + ix);
+    const float4 lo = __ldg(b), hi = __ldg(b + pxy);
+    const float c00 = fmaf(ax, lo.y - lo.x, lo.x), c01 = fmaf(ax, lo.w - lo.z, lo.z);
+    const float c10 = fmaf(ax, hi.y - hi.x, hi.x), c11 = fmaf(ax, hi.w - hi.z, hi.z);
+    const float c0 = fmaf(ay, c01 - c00, c00), c1 = fmaf(ay, c11 - c10, c10);
+    return fmaf(az, c1 - c0, c0);
+  }
+};
+
 // Texture coordinates: the ray set-up already added the 1/2 texel offset.
 struct TexSampler {
   cudaTextureObject_t tex;
@@ -83,6 +106,26 @@ __global__ void __launch_bounds__(kFPThreads) fp_soft_kernel(RayParams rp, const
     const RaySetup rs = setup_ray(rp, views[n], u, v);
     SoftSampler<T> smp;
     smp.vol = vpad + b * pad_elems;
+    smp.px = rp.nx + 2 * kPad;
+    smp.pxy = smp.px * (rp.ny + 2 * kPad);
+    smp.mx = (float)rp.nx; smp.my = (float)rp.ny; smp.mz = (float)rp.nz;
+    const float val = rs.count > 0 ? ray_sum(smp, rs) * rp.scale : 0.f;
+    fp_store(rp, o, n, b, u, v, val, res);
+  }
+  if (o.abs_sum) block_add_double((double)fabsf(res), o.abs_sum);
+}
+
+__global__ void __launch_bounds__(kFPThreads) fp_quad_kernel(RayParams rp, const FPView* __restrict__ views,
+                                                             const float4* __restrict__ quads,
+                                                             int64_t pad_elems, FPOut o) {
+  int u, v;
+  tile_pixel(rp, u, v);
+  const int n = blockIdx.y, b = blockIdx.z;
+  float res = 0.f;
+  if (u < rp.nu && v < rp.nv) {
+    const RaySetup rs = setup_ray(rp, views[n], u, v);
+    QuadSampler smp;
+    smp.q = quads + b * pad_elems;
     smp.px = rp.nx + 2 * kPad;
     smp.pxy = smp.px * (rp.ny + 2 * kPad);
     smp.mx = (float)rp.nx; smp.my = (float)rp.ny; smp.mz = (float)rp.nz;
@@ -197,11 +240,42 @@ static int grid_for(int64_t n, int threads = 256) {
   return (int)std::min<int64_t>(b, 148 * 16);
 }
 
+// Quad records (padded indexing, border kPad) of one volume: only records that
+// reach an interior voxel are written; the others stay zero from the plan's
+// initial clear. grid: (x, y) tiles of 32 x 8, z planes.
+template <class Tin>
+__global__ void __launch_bounds__(256) stage_quads_kernel(const Tin* __restrict__ in,
+                                                          float4* __restrict__ q, int nx, int ny,
+                                                          int nz) {
+  const int x = blockIdx.x * 32 + (threadIdx.x & 31) + kPad - 1;  // padded x in [kPad-1, kPad+nx)
+  const int y = blockIdx.y * 8 + (threadIdx.x >> 5) + kPad - 1;
+  const int z = blockIdx.z + kPad;
+  if (x >= kPad + nx || y >= kPad + ny) return;
+  const int px = nx + 2 * kPad, py = ny + 2 * kPad;
+  const Tin* plane = in + (int64_t)(z - kPad) * nx * ny;
+  auto at = [&](int xx, int yy) {
+    const int ox = xx - kPad, oy = yy - kPad;
+    return (ox >= 0 && ox < nx && oy >= 0 && oy < ny) ? load_as_float(plane, (int64_t)oy * nx + ox)
+                                                      : 0.f;
+  };
+  q[((int64_t)z * py + y) * px + x] = make_float4(at(x, y), at(x + 1, y), at(x, y + 1),
+                                                  at(x + 1, y + 1));
+}
+
 template <class Tin>
 static int stage_volume_soft(Plan* p, const Tin* vol, int batch, cudaStream_t st) {
   const GeomParams& g = p->gp;
   const int64_t vox = (int64_t)g.nx * g.ny * g.nz;
   dim3 grid(grid_for(vox), batch);
+  if (p->d_vol_quads) {
+    dim3 qg((g.nx + 1 + 31) / 32, (g.ny + 1 + 7) / 8, g.nz);
+    for (int b = 0; b < batch; ++b) {
+      stage_quads_kernel<Tin><<<qg, 256, 0, st>>>(vol + b * vox, p->d_vol_quads + b * p->pad_elems,
+                                                  g.nx, g.ny, g.nz); note_launch();
+      DTV_LAUNCH_CHECK();
+    }
+    return DTV_OK;
+  }
   if (p->stage_dtype == DTV_F16) {
     stage_pad_kernel<Tin, __half><<<grid, 256, 0, st>>>(vol, (__half*)p->d_vol_pad, g.nx, g.ny, g.nz,
                                                         p->pad_elems); note_launch();
@@ -284,6 +358,8 @@ int forward_impl(Plan* p, const void* vol, int vol_dtype, int batch, float* out,
     fp_pair_kernel<<<grid, kFPThreads, 0, st>>>(rp, p->d_fpv, p->pair_tex_dev, o); note_launch();
   } else if (tex) {
     fp_tex_kernel<<<grid, kFPThreads, 0, st>>>(rp, p->d_fpv, p->vol_tex_dev, o); note_launch();
+  } else if (p->d_vol_quads) {
+    fp_quad_kernel<<<grid, kFPThreads, 0, st>>>(rp, p->d_fpv, p->d_vol_quads, p->pad_elems, o); note_launch();
   } else if (p->stage_dtype == DTV_F16) {
     fp_soft_kernel<__half><<<grid, kFPThreads, 0, st>>>(rp, p->d_fpv, (const __half*)p->d_vol_pad,
                                                         p->pad_elems, o); note_launch();

@@ -60,6 +60,7 @@ void free_plan(Plan* p) {
   cudaFree(p->d_bpv);
   free(p->h_bpv);
   cudaFree(p->d_vol_pad);
+  cudaFree(p->d_vol_quads);
   cudaFree(p->d_sino_pad);
   delete p;
 }
@@ -143,9 +144,17 @@ int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Pla
   p->stage_dtype = (flags & DTV_PLAN_STAGE_F16) ? DTV_F16 : DTV_F32;
   p->pad_elems = (int64_t)(gp.nx + 2 * kPad) * (gp.ny + 2 * kPad) * (gp.nz + 2 * kPad);
   const size_t esz = p->stage_dtype == DTV_F16 ? 2 : 4;
-  // Staged volumes: zero border written once here, interiors by each call.
-  PLAN_CUDA(cudaMalloc(&p->d_vol_pad, esz * p->pad_elems * max_batch));
-  PLAN_CUDA(cudaMemset(p->d_vol_pad, 0, esz * p->pad_elems * max_batch));
+  // Staged volumes of the software sampler (FP32: quad records, FP16: the
+  // padded volume): zero border written once here, interiors by each call.
+  if (!(flags & (DTV_PLAN_TEX | DTV_PLAN_TEX_PAIRS))) {
+    if (p->stage_dtype == DTV_F32) {
+      PLAN_CUDA(cudaMalloc(&p->d_vol_quads, sizeof(float4) * p->pad_elems * max_batch));
+      PLAN_CUDA(cudaMemset(p->d_vol_quads, 0, sizeof(float4) * p->pad_elems * max_batch));
+    } else {
+      PLAN_CUDA(cudaMalloc(&p->d_vol_pad, esz * p->pad_elems * max_batch));
+      PLAN_CUDA(cudaMemset(p->d_vol_pad, 0, esz * p->pad_elems * max_batch));
+    }
+  }
   const int64_t sino_pad = (int64_t)(gp.nu + 2 * kPad) * (gp.nv + 2 * kPad) * gp.n_views;
   PLAN_CUDA(cudaMalloc(&p->d_sino_pad, sizeof(float) * sino_pad));
   PLAN_CUDA(cudaMemset(p->d_sino_pad, 0, sizeof(float) * sino_pad));
