@@ -1,3 +1,4 @@
+#include <algorithm>
 // Plans (device tables + sampler staging) and the projector entry points.
 #include <stdlib.h>
 #include <string.h>
@@ -413,6 +414,11 @@ int dtv_forward_many(dtv_plan* const* plans, const void* const* vols, int32_t vo
     DTV_CHECK(ps[k]->flags & DTV_PLAN_TEX_PAIRS, "plan %d is not a DTV_PLAN_TEX_PAIRS plan", k);
     DTV_CHECK(ps[k]->device == ps[0]->device, "plans %d and 0 are on different devices", k);
   }
+  // each plan stages its one volume into its own texture: a plan may appear once
+  std::vector<Plan*> sorted(ps);
+  std::sort(sorted.begin(), sorted.end());
+  DTV_CHECK(std::adjacent_find(sorted.begin(), sorted.end()) == sorted.end(),
+            "a plan appears more than once");
   DeviceGuard dg(ps[0]->device);
   return forward_many_impl(ps.data(), vols, vol_dtype, outs, count, epilogue, gs, sigma,
                            as_stream(stream));
@@ -430,6 +436,10 @@ int dtv_backward_many(dtv_plan* const* plans, const float* const* sinos, float* 
               "plan %d has no sinogram texture (DTV_PLAN_TEX or DTV_PLAN_TEX_PAIRS)", k);
     DTV_CHECK(ps[k]->device == ps[0]->device, "plans %d and 0 are on different devices", k);
   }
+  std::vector<Plan*> sorted(ps);
+  std::sort(sorted.begin(), sorted.end());
+  DTV_CHECK(std::adjacent_find(sorted.begin(), sorted.end()) == sorted.end(),
+            "a plan appears more than once");
   DeviceGuard dg(ps[0]->device);
   return backward_many_impl(ps.data(), sinos, outs, count, accumulate ? 1 : 0, as_stream(stream));
 }

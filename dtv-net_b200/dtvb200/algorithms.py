@@ -98,6 +98,11 @@ class Batched:
 
     def __init__(self, algs, use_graph: bool = True):
         self.algs = list(algs)
+        plans = [id(a.plan) for a in self.algs]
+        if len(set(plans)) != len(plans):
+            # a plan stages its input in buffers of its own; two streams using
+            # one plan at once would overwrite each other's staging
+            raise ValueError("each reconstruction of a Batched set needs a plan of its own")
         self.use_graph = use_graph
         self.launches_per_run = 0
         self._streams = None
@@ -319,6 +324,8 @@ class BatchedFISTA:
     def __init__(self, plans, cascades: int = 30, lamb: float = 10e3, L: float = 0.0001,
                  use_graph: bool = True):
         self.plans = list(plans)
+        if len({id(p) for p in self.plans}) != len(self.plans):
+            raise ValueError("each reconstruction needs a plan of its own")
         self.cascades = int(cascades)
         self.lamb, self.L = float(lamb), float(L)
         self.use_graph = use_graph

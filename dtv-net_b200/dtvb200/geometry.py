@@ -144,8 +144,12 @@ class Plan:
     tiles still uses the texture unit). The backprojector samples the
     sinogram through a texture for "tex", "pairs" and "tma".
     ``stage_f16`` stages projected volumes as FP16 ("soft"/"tex").
-    ``adjoint`` keeps a per-ray table that speeds up :meth:`adjoint`
-    (32 bytes per ray and view)."""
+    ``adjoint`` keeps a per-ray table (32 bytes per ray and view) and cell
+    records (16 bytes per voxel) that speed up :meth:`adjoint`.
+
+    A plan stages its input in buffers of its own, so its calls are ordered
+    on the stream they are made on; calls of one plan from two streams at once
+    race. Use one plan per concurrent stream."""
 
     def __init__(self, geometry: Geometry, max_batch: int = 1, sampler: str = "soft",
                  stage_f16: bool = False, device=None, adjoint: bool = False):

@@ -201,13 +201,15 @@ DTV_API int dtv_plan_fp_samples(const dtv_plan* plan, double* samples_per_volume
  * the reference, which launched per view): plans[k] projects vols[k] (one
  * volume each, any size and view count) into outs[k], with the epilogue of
  * dtv_forward against gs[k] (no abs_sum). DTV_PLAN_TEX_PAIRS plans on one
- * device; the per-ray sums equal those of dtv_forward. Up to 24 plans share a
- * launch, more take further launches. */
+ * device, each at most once (a plan stages its volume into its own texture);
+ * the per-ray sums equal those of dtv_forward. Up to 24 plans share a launch,
+ * more take further launches. */
 DTV_API int dtv_forward_many(dtv_plan* const* plans, const void* const* vols, int32_t vol_dtype,
                              float* const* outs, int32_t count, int32_t epilogue,
                              const float* const* gs, float sigma, void* stream);
 /* Several plans' FDK backprojections in one launch (plans with a sinogram
- * texture: DTV_PLAN_TEX or DTV_PLAN_TEX_PAIRS); values equal dtv_backward's. */
+ * texture: DTV_PLAN_TEX or DTV_PLAN_TEX_PAIRS, each at most once); values equal
+ * dtv_backward's. */
 DTV_API int dtv_backward_many(dtv_plan* const* plans, const float* const* sinos,
                               float* const* outs, int32_t count, int32_t accumulate, void* stream);
 

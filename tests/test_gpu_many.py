@@ -80,6 +80,11 @@ def test_many_rejects_unsupported_plans(cuda):
         dtvb200.backward_many([soft], [torch.zeros(soft.sino_shape(1), device=cuda)])
     with pytest.raises(ValueError):
         dtvb200.forward_many([], [])
+    with pytest.raises(dtvb200.DtvError):  # one staging texture per plan
+        dtvb200.forward_many([plans[0], plans[0]], [vols[0], vols[0]])
+    sino = torch.zeros(plans[0].sino_shape(1), device=cuda)
+    with pytest.raises(dtvb200.DtvError):
+        dtvb200.backward_many([plans[0], plans[0]], [sino, sino])
 
 
 @pytest.mark.parametrize("graph", [False, True])
