@@ -85,6 +85,10 @@ def test_many_rejects_unsupported_plans(cuda):
     sino = torch.zeros(plans[0].sino_shape(1), device=cuda)
     with pytest.raises(dtvb200.DtvError):
         dtvb200.backward_many([plans[0], plans[0]], [sino, sino])
+    with pytest.raises(ValueError):
+        dtvb200.BatchedFISTA([plans[0], plans[0]], 2)
+    with pytest.raises(ValueError):
+        dtvb200.Batched([dtvb200.FISTA(plans[0], 2), dtvb200.FISTA(plans[0], 2)])
 
 
 @pytest.mark.parametrize("graph", [False, True])
