@@ -525,6 +525,7 @@ def run_train(args):
     from dtvb200.nets import UnrolledPDHG
     from dtvb200.phantom import ellipsoids
     dev = torch.device("cuda", 0)
+    torch.backends.cudnn.benchmark = True  # the conv shapes repeat every stage
     n, views, det, stages = 128, 48, 192, 10
     ang = np.linspace(0, 360, views, endpoint=False)
     geo = dtvb200.circular(ang, (n, n, n), (1.0,) * 3, (det, det), (1.5, 1.5), 500.0, 1000.0)

@@ -7,7 +7,8 @@ the forward projector with the FDK backprojector as its "gradient"
 pass go through the matched adjoint (dtv_backward_adjoint), so the gradients
 are exact; each stage is checkpointed (its activations are recomputed in the
 backward pass), and the convolution blocks run their activations in BF16 under
-autocast while their weights stay FP32.
+autocast while their weights stay FP32, in the channels-last 3-D layout that
+cuDNN's tensor-core convolutions take without transposes.
 """
 from __future__ import annotations
 
@@ -52,11 +53,16 @@ class UnrolledPDHG(nn.Module):
         self.tau = nn.Parameter(torch.full((stages,), float(tau)))
         self.checkpoint_stages = checkpoint_stages
         self.bf16 = bf16
+        self._channels_last()
+
+    def _channels_last(self):
+        for b in self.blocks:
+            b.to(memory_format=torch.channels_last_3d)
 
     def stage(self, s: int, x: torch.Tensor, p: torch.Tensor) -> torch.Tensor:
         grad = self.BP.apply(self.FP.apply(x) - p)
         with torch.autocast("cuda", dtype=torch.bfloat16, enabled=self.bf16):
-            r = self.blocks[s](x)
+            r = self.blocks[s](x.to(memory_format=torch.channels_last_3d))
         return x - self.lamb[s] * grad - self.tau[s] * r.float()
 
     def forward(self, x0: torch.Tensor, p: torch.Tensor, return_all: bool = False):
@@ -83,6 +89,7 @@ class LEARN(UnrolledPDHG):
             nn.Conv3d(1, 8, 3, padding=1), nn.ReLU(), nn.Conv3d(8, 8, 3, padding=1), nn.ReLU(),
             nn.Conv3d(8, 8, 3, padding=1), nn.ReLU(), nn.Conv3d(8, 1, 3, padding=1))
         self.blocks = nn.ModuleList([dual] * cascades)
+        self._channels_last()
 
     def forward(self, image, sino):
         return super().forward(image, sino, return_all=True)
