@@ -629,6 +629,10 @@ def run_fista64(args):
     _, plain = build("soft", False)
     plain()
     ps = time_steps(plain, args.steps, stream)
+    cpu = None
+    if not args.no_cpu:
+        cpu = fista64_cpu(c, truth[0, 0].double().cpu().numpy(), dtv_params(plan, dev)["sigma"],
+                          tuple(power_norm((64, 64, 64), a, False, device=dev) for a in range(3)))
     line = {
         "metric": METRIC, "value": units * args.steps / secs / 1e9, "unit": UNIT, "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
@@ -642,9 +646,34 @@ def run_fista64(args):
                              "sampler": "soft"},
         "gpu_launches": launches * args.steps,
         "clocks": clk.summary(),
+        "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def fista64_cpu(c, truth_np, sigma, v):
+    """The whole 64^3 step (FP, BP, 20 FISTA-DTV iterations) by the FP64
+    oracle on all host cores, timed once."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as O
+    ang = np.linspace(0, 360, c["n_views"], endpoint=False)
+    og = O.circular_geometry(ang, (c["nx"], c["ny"], c["nz"]), (c["voxel"],) * 3,
+                             (c["nu"], c["nv"]), (c["pitch"], c["pitch"]), c["sod"], c["sdd"])
+    vol = np.ascontiguousarray(truth_np, dtype=np.float64)
+    fp = lambda x: O.forward(og, x).reshape(x.shape[0], 1, *og.sino_shape)  # noqa: E731
+    bp = lambda s: O.backward(og, s).reshape(s.shape[0], 1, *og.vol_shape)  # noqa: E731
+    t0 = time.perf_counter()
+    sino = fp(vol.reshape(1, 1, *vol.shape))
+    bp(sino)
+    O.dtvfista_run(fp, bp, np.zeros((1, 1) + og.vol_shape), sino, (c["nx"], c["ny"], c["nz"]),
+                   c["iters"], sigma, v, (1e-3,) * 3, quirk=False)
+    secs = time.perf_counter() - t0
+    units = (c["iters"] + 1) * (O.fp_samples(og) + c["nx"] * c["ny"] * c["nz"] * c["n_views"])
+    return {"value": units / secs / 1e9, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+            "recon_per_s": 1.0 / secs,
+            "sample": "the whole step (FP + BP + 20 FISTA-DTV iterations), FP64 oracle, once"}
 
 
 def run_large512(args):
