@@ -649,6 +649,36 @@ __global__ void fista_kernel(float* __restrict__ y, float* __restrict__ xp, cons
   }
 }
 
+// The same update for several volumes in one launch: a flat index over the
+// volumes' elements, each thread finding its volume from the prefix offsets
+// held in the launch parameters.
+constexpr int kFistaMany = 64;
+struct FistaMany {
+  float* y[kFistaMany];
+  float* xp[kFistaMany];
+  const float* bp[kFistaMany];
+  int64_t start[kFistaMany + 1];
+  int count;
+};
+
+__global__ void fista_many_kernel(const __grid_constant__ FistaMany m, float L, float thr,
+                                  float mom) {
+  const int64_t total = m.start[m.count];
+  int k = 0;
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < total;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    while (g >= m.start[k + 1]) ++k;  // g only grows within a thread
+    const int64_t t = g - m.start[k];
+    float* y = m.y[k];
+    float* xp = m.xp[k];
+    const float dd = y[t] - L * m.bp[k][t];
+    const float mm = fmaxf(fabsf(dd) - thr, 0.f);
+    const float xi = dd > 0.f ? mm : (dd < 0.f ? -mm : 0.f);
+    y[t] = xi + mom * (xi - xp[t]);
+    xp[t] = xi;
+  }
+}
+
 // ---- FISTA-DTV (DTVFISTA.py:29-38) -------------------------------------------------------------------
 __global__ void relu_step_kernel(const float* __restrict__ f, const float* bp, float* z, int64_t n,
                                  float sigma) {
@@ -923,6 +953,30 @@ int dtv_fista_update(float* y, float* x_prev, const float* bp, int64_t n, float 
   DTV_CHECK(y && x_prev && bp && n > 0, "bad argument");
   fista_kernel<<<blocks_for(n), 256, 0, as_stream(stream)>>>(y, x_prev, bp, n, L, thresh, momentum); note_launch();
   DTV_LAUNCH_CHECK();
+  return DTV_OK;
+}
+
+int dtv_fista_update_many(float* const* y, float* const* x_prev, const float* const* bp,
+                          const int64_t* n, int32_t count, float L, float thresh, float momentum,
+                          void* stream) {
+  DTV_CHECK(y && x_prev && bp && n && count >= 1, "bad argument");
+  FistaMany m;
+  for (int c0 = 0; c0 < count; c0 += kFistaMany) {
+    const int cnt = std::min(kFistaMany, count - c0);
+    m.count = cnt;
+    m.start[0] = 0;
+    for (int k = 0; k < cnt; ++k) {
+      DTV_CHECK(y[c0 + k] && x_prev[c0 + k] && bp[c0 + k] && n[c0 + k] > 0, "bad volume %d",
+                c0 + k);
+      m.y[k] = y[c0 + k];
+      m.xp[k] = x_prev[c0 + k];
+      m.bp[k] = bp[c0 + k];
+      m.start[k + 1] = m.start[k] + n[c0 + k];
+    }
+    fista_many_kernel<<<blocks_for(m.start[cnt]), 256, 0, as_stream(stream)>>>(m, L, thresh,
+                                                                                momentum); note_launch();
+    DTV_LAUNCH_CHECK();
+  }
   return DTV_OK;
 }
 

@@ -78,6 +78,7 @@ SIGNATURES = {
     "dtv_plan_device_status": [_P, _IP, _I],
     "dtv_fbp_filter": [_P, _P, ctypes.c_int64, _I, _I, _F, _F, _F, _I, _P],
     "dtv_forward_many": [_P, _P, _I, _P, _I, _I, _P, _F, _P],
+    "dtv_fista_update_many": [_P, _P, _P, _P, _I, _F, _F, _F, _P],
     "dtv_backward_many": [_P, _P, _P, _I, _I, _P],
     "dtv_plan_fp_samples": [_P, _DP],
     "dtv_forward": [_P, _P, _I, _I, _P, _I, _P, _F, _P, _P],

@@ -315,9 +315,9 @@ class FISTA(_Graphable):
 
 class BatchedFISTA:
     """:class:`FISTA` on several reconstructions in lockstep: per iteration one
-    forward-projector launch and one backprojector launch cover every volume,
-    whatever their sizes and view counts (dtv_forward_many / dtv_backward_many),
-    followed by the per-volume momentum updates. With ``use_graph`` a whole run
+    forward-projector launch, one backprojector launch and one update launch
+    cover every volume, whatever their sizes and view counts
+    (dtv_forward_many, dtv_backward_many, dtv_fista_update_many). With ``use_graph`` a whole run
     is one captured CUDA graph. The plans must be "pairs" (or "tma") plans;
     each reconstruction gives the same result as its own :class:`FISTA` run."""
 
@@ -352,6 +352,10 @@ class BatchedFISTA:
     def _enqueue(self, st):
         stream = _stream(st[0]["y"].device)
         ys, rs, gs, bps = ([d[k] for d in st] for k in ("y", "r", "g", "bp"))
+        vp = ctypes.c_void_p * len(st)
+        upd = (vp(*[d["y"].data_ptr() for d in st]), vp(*[d["xp"].data_ptr() for d in st]),
+               vp(*[d["bp"].data_ptr() for d in st]),
+               (ctypes.c_int64 * len(st))(*[d["y"].numel() for d in st]))
         for d in st:
             d["y"].copy_(d["img"])
             d["xp"].copy_(d["img"])
@@ -360,9 +364,8 @@ class BatchedFISTA:
             forward_many(self.plans, ys, rs, epilogue=_lib.DTV_EPI_RESIDUAL, gs=gs)
             backward_many(self.plans, rs, bps)
             tp = (1 + math.sqrt(1 + 4 * t ** 2)) / 2
-            for d in st:
-                call("dtv_fista_update", _ptr(d["y"]), _ptr(d["xp"]), _ptr(d["bp"]),
-                     d["y"].numel(), self.L, self.lamb * self.L, (t - 1) / tp, stream)
+            call("dtv_fista_update_many", *upd, len(st), self.L, self.lamb * self.L,
+                 (t - 1) / tp, stream)
             t = tp
 
     def run(self, images, sinos, outs=None):

@@ -342,6 +342,12 @@ DTV_API int dtv_pdhg_primal(float* f, void* fbar, const float* recon, float* p, 
  * x_prev = x. n elements, all f32. */
 DTV_API int dtv_fista_update(float* y, float* x_prev, const float* bp, int64_t n, float L, float thresh,
                      float momentum, void* stream);
+/* dtv_fista_update for several volumes (y[k], x_prev[k], bp[k] of n[k]
+ * elements) with one L, threshold and momentum, in one launch. No counterpart
+ * in the reference. */
+DTV_API int dtv_fista_update_many(float* const* y, float* const* x_prev, const float* const* bp,
+                                  const int64_t* n, int32_t count, float L, float thresh,
+                                  float momentum, void* stream);
 
 /* ---- FISTA-DTV (model/FISTA/DTVFISTA.py:23-43) ---------------------------------- */
 /* z = relu(f - sigma*bp) (z may alias bp). */
