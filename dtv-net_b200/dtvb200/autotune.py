@@ -15,6 +15,11 @@ tile and on the geometry (magnification, pixel pitch, volume aspect).
 DTV_TUNE_FP_TEX_SHARE applies to "tma" plans: of every 8 ray tiles, that
 many sample through the texture unit and the rest from shared memory, so the
 texture pipe and the shared-memory/FMA pipes work side by side.
+
+DTV_TUNE_ADJOINT applies to plans with adjoint tables: the exact adjoint
+scatters either per 16^3 brick through shared-memory atomics (0) or into
+per-cell records with 16-byte vector atomics in L2 (1); which is faster
+depends on whether the records fit in L2. It is timed on plan.adjoint.
 """
 from __future__ import annotations
 
@@ -25,7 +30,8 @@ from .geometry import Plan
 
 _CACHE: dict = {}
 N_RAY_TILES = 8
-CANDIDATES = {_lib.DTV_TUNE_FP_RAY_TILE: range(N_RAY_TILES), _lib.DTV_TUNE_FP_TEX_SHARE: range(9)}
+CANDIDATES = {_lib.DTV_TUNE_FP_RAY_TILE: range(N_RAY_TILES), _lib.DTV_TUNE_FP_TEX_SHARE: range(9),
+              _lib.DTV_TUNE_ADJOINT: range(2)}
 
 
 def _key(plan: Plan, batch: int, key: int):
@@ -33,22 +39,26 @@ def _key(plan: Plan, batch: int, key: int):
             plan.geometry.key(), int(key))
 
 
-def time_forward(plan: Plan, vol: torch.Tensor, out: torch.Tensor, reps: int = 5,
-                 warmup: int = 2) -> float:
-    """Median milliseconds of ``plan.forward(vol, out)`` on the current stream."""
+def _median_ms(plan: Plan, fn, reps: int, warmup: int) -> float:
     with torch.cuda.device(plan.device):
         for _ in range(warmup):
-            plan.forward(vol, out)
+            fn()
         times = []
         for _ in range(reps):
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record()
-            plan.forward(vol, out)
+            fn()
             b.record()
             b.synchronize()
             times.append(a.elapsed_time(b))
     times.sort()
     return times[len(times) // 2]
+
+
+def time_forward(plan: Plan, vol: torch.Tensor, out: torch.Tensor, reps: int = 5,
+                 warmup: int = 2) -> float:
+    """Median milliseconds of ``plan.forward(vol, out)`` on the current stream."""
+    return _median_ms(plan, lambda: plan.forward(vol, out), reps, warmup)
 
 
 def tune(plan: Plan, batch: int = 1, key: int = None, candidates=None,
@@ -71,11 +81,15 @@ def tune(plan: Plan, batch: int = 1, key: int = None, candidates=None,
         candidates = CANDIDATES[key]
     gen = torch.Generator(device=plan.device).manual_seed(0)
     vol = torch.rand(plan.vol_shape(batch), device=plan.device, generator=gen)
-    out = torch.empty(plan.sino_shape(batch), device=plan.device)
+    sino = torch.rand(plan.sino_shape(batch), device=plan.device, generator=gen)
+    if key == _lib.DTV_TUNE_ADJOINT:
+        fn = lambda: plan.adjoint(sino, vol)  # noqa: E731
+    else:
+        fn = lambda: plan.forward(vol, sino)  # noqa: E731
     times = {}
     for c in candidates:
         plan.set_tuning(key, int(c))
-        times[int(c)] = time_forward(plan, vol, out, reps, warmup)
+        times[int(c)] = _median_ms(plan, fn, reps, warmup)
     best = min(times, key=times.get)
     plan.set_tuning(key, best)
     _CACHE[ck] = (best, dict(times))

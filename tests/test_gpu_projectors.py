@@ -164,6 +164,10 @@ def test_tuning_keys_and_autotune(cuda):
     other = dtvb200.Plan(g, sampler="pairs", device=cuda)
     assert dtvb200.autotune.tune(other) == times  # cached: applied without timing
     assert other.get_tuning(key) == plan.get_tuning(key)
+    adj = dtvb200.Plan(g, device=cuda, adjoint=True)
+    t_adj = dtvb200.autotune.tune(adj, key=_lib.DTV_TUNE_ADJOINT, reps=2, warmup=1)
+    assert sorted(t_adj) == [0, 1]
+    assert adj.get_tuning(_lib.DTV_TUNE_ADJOINT) == min(t_adj, key=t_adj.get)
 
 
 @pytest.mark.parametrize("kind", KINDS)
