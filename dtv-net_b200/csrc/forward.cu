@@ -622,7 +622,8 @@ __global__ void __launch_bounds__(256) adjoint_cells_kernel(RayParams rp,
                                                             const FPView* __restrict__ views,
                                                             const float4* __restrict__ rays,
                                                             const float* __restrict__ sino,
-                                                            float4* __restrict__ cells, int batch) {
+                                                            float4* __restrict__ cells, int batch,
+                                                            int zb0, int zb1) {
   const int64_t per = (int64_t)rp.n_views * rp.nu * rp.nv;
   const int64_t total = per * batch;
   const int cx = rp.nx + 1, cy = rp.ny + 1;
@@ -645,13 +646,23 @@ __global__ void __launch_bounds__(256) adjoint_cells_kernel(RayParams rp,
       rs = setup_ray(rp, views[(int)(q / rp.nv)], u, (int)(q % rp.nv));
     }
     float4* cb = cells + b * citem;
-    for (int k = 0; k < rs.count; ++k) {
+    // this launch takes the samples whose base z-cell is in [zb0, zb1): their
+    // k range from the ray's (monotone) z, widened by one, then tested exactly
+    int k0 = 0, k1 = rs.count;
+    if (rs.dp[2] != 0.f) {
+      const float inv = 1.f / rs.dp[2];
+      const float ka = ((float)zb0 - rs.p0[2]) * inv, kb = ((float)zb1 - rs.p0[2]) * inv;
+      const float cnt = (float)rs.count;  // clamp in float: the estimates may be huge
+      k0 = (int)fminf(fmaxf(floorf(fminf(ka, kb)) - 1.f, 0.f), cnt);
+      k1 = (int)fminf(fmaxf(ceilf(fmaxf(ka, kb)) + 1.f, 0.f), cnt);
+    }
+    for (int k = k0; k < k1; ++k) {
       const float kf = (float)k;
       const float x = fmaf(kf, rs.dp[0], rs.p0[0]), y = fmaf(kf, rs.dp[1], rs.p0[1]),
                   z = fmaf(kf, rs.dp[2], rs.p0[2]);
       const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
       const int ix = (int)fx, iy = (int)fy, iz = (int)fz;
-      if (ix < -1 || ix > rp.nx - 1 || iy < -1 || iy > rp.ny - 1 || iz < -1 || iz > rp.nz - 1)
+      if (iz < zb0 || iz >= zb1 || ix < -1 || ix > rp.nx - 1 || iy < -1 || iy > rp.ny - 1)
         continue;
       const float ax = x - fx, ay = y - fy, az = z - fz;
       const float bx = 1.f - ax, by = 1.f - ay;
@@ -699,9 +710,16 @@ int adjoint_impl(Plan* p, const float* sino, int batch, float* out, cudaStream_t
     DTV_CUDA_TRY(cudaMemsetAsync(p->d_cells, 0, cells * sizeof(float4), st));
     const int64_t rays = (int64_t)gp.n_views * gp.nu * gp.nv * batch;
     const int grid = (int)std::min<int64_t>((rays + 255) / 256, 148LL * 64);
-    adjoint_cells_kernel<<<grid, 256, 0, st>>>(rp, p->d_fpv, p->d_rays, sino, p->d_cells,
-                                               batch); note_launch();
-    DTV_LAUNCH_CHECK();
+    // z-slabs of base cells whose records (at most 72 MB over the batch) stay
+    // resident in L2 while their samples scatter; base cells run over [-1, nz-1]
+    const int64_t plane_bytes = (int64_t)(gp.nx + 1) * (gp.ny + 1) * sizeof(float4) * batch;
+    const int slab = (int)std::max<int64_t>(1, (72LL << 20) / plane_bytes);
+    for (int zb0 = -1; zb0 < gp.nz; zb0 += slab) {
+      const int zb1 = std::min(zb0 + slab, gp.nz);
+      adjoint_cells_kernel<<<grid, 256, 0, st>>>(rp, p->d_fpv, p->d_rays, sino, p->d_cells, batch,
+                                                 zb0, zb1); note_launch();
+      DTV_LAUNCH_CHECK();
+    }
     const int ggrid = (int)std::min<int64_t>((vox * batch + 255) / 256, 148LL * 32);
     adjoint_gather_kernel<<<ggrid, 256, 0, st>>>(p->d_cells, out, gp.nx, gp.ny, gp.nz, batch); note_launch();
     DTV_LAUNCH_CHECK();
