@@ -251,9 +251,11 @@ int dtv_geometry_vector(dtv_geometry* g, double* views, const float* pv, int32_t
   g->fp_step = 1.0;                           // forwardKernel.cu:72
   g->fp_scale = 1.0;
   g->fp_phase = DTV_PHASE_VECTOR;
-  g->bp_weight_power = 1;                              // backwardKernel.cu:171
-  g->bp_scale = n >= 21 ? 2.0 * kRefPi / (n / 21) : 0.0;  // backwardKernel.cu:177,230
-  g->bp_extent_check = 1;                              // backwardKernel.cu:172
+  g->bp_weight_power = 1;                              // backwardKernel.cu:37
+  // backwardKernel.cu:43,96: 2*pi / (N / 21) in integer division. With fewer than
+  // 21 views the reference divides by zero; the scale is 0 here instead.
+  g->bp_scale = n >= 21 ? 2.0 * kRefPi / (n / 21) : 0.0;
+  g->bp_extent_check = 1;                              // backwardKernel.cu:38
   for (int a = 0; a < n; ++a) {
     const float* p = pv + 12 * a;
     double* o = views + 12 * a;

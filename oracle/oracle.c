@@ -265,13 +265,13 @@ static inline double det3(const double* a, const double* b, const double* c) {
 }
 
 /* Vector-geometry backprojector, model/ConeBeamLayers/Beijing/plug/kernel/
- * backwardKernel.cu:18-45 (kernel) and :205-231 (host), for any view count
+ * backwardKernel.cu:18-45 (kernel) and :47-104 (host), for any view count
  * (the reference requires a multiple of 1512 through its texture chunking). */
 void oracle_backward_vector_literal(const double* sino, int batch, const double* pv, int n_views,
                                     int X, int Y, int Z, int W, int H, int q, double* vol) {
-  const double vcx = X / -2.0, vcy = Y / -2.0, vcz = Z / -2.0; /* :207 */
-  const double dcx = W / -2.0, dcy = H / -2.0;                 /* :208 */
-  const int blocks = n_views / 21;                             /* :230 angles/21 */
+  const double vcx = X / -2.0, vcy = Y / -2.0, vcz = Z / -2.0; /* :73 */
+  const double dcx = W / -2.0, dcy = H / -2.0;                 /* :74 */
+  const int blocks = n_views / 21;                             /* :96 angles/21 */
   memset(vol, 0, sizeof(double) * (size_t)batch * X * Y * Z);
 #pragma omp parallel for collapse(3) schedule(static)
   for (int b = 0; b < batch; ++b)
@@ -280,32 +280,32 @@ void oracle_backward_vector_literal(const double* sino, int batch, const double*
         double* Vb = vol + (int64_t)b * X * Y * Z;
         for (int k = 0; k < Z; ++k) {
           double acc_all = 0.0;
-          for (int a0 = 0; a0 < n_views; a0 += 21) { /* one launch per 21 views (:229-231) */
+          for (int a0 = 0; a0 < n_views; a0 += 21) { /* one launch per 21 views (:95-96) */
             double value = 0.0;
             int found = 0;
-            for (int a = a0; a < a0 + 21 && a < n_views; ++a) { /* :162 */
+            for (int a = a0; a < a0 + 21 && a < n_views; ++a) { /* :28 */
               const double* P = pv + 12 * a;
               double s[3] = {P[0], P[1], -P[2]}, d[3] = {P[3], P[4], -P[5]};
               double vv[3] = {P[6], P[7], P[8]}, uu[3] = {P[9], P[10], P[11]};
-              double c[3] = {vcx + x, vcy + y, vcz + k}; /* :167 */
+              double c[3] = {vcx + x, vcy + y, vcz + k}; /* :33 */
               double smc[3], cms[3], smd[3];
               for (int t = 0; t < 3; ++t) {
                 smc[t] = s[t] - c[t];
                 cms[t] = c[t] - s[t];
                 smd[t] = s[t] - d[t];
               }
-              double fs = 1.0 / det3(uu, vv, smc);            /* :168 */
-              double dX = fs * det3(cms, vv, smd) - dcx;       /* :169 */
-              double dY = fs * det3(uu, cms, smd) - dcy;       /* :170 */
-              double fr = fs * det3(uu, vv, smd);              /* :171 */
-              if (dX < -1 || dX > X + 1 || dY < -1 || dY > Y + 1) continue; /* :172 */
+              double fs = 1.0 / det3(uu, vv, smc);            /* :34 */
+              double dX = fs * det3(cms, vv, smd) - dcx;       /* :35 */
+              double dY = fs * det3(uu, cms, smd) - dcy;       /* :36 */
+              double fr = fs * det3(uu, vv, smd);              /* :37 */
+              if (dX < -1 || dX > X + 1 || dY < -1 || dY > Y + 1) continue; /* :38 */
               found = 1;
               /* tex3D(sino, dX, dY, a%TEXA+0.5): texel coordinate dX is pixel
-               * coordinate dX-0.5 (:174) */
+               * coordinate dX-0.5 (:40) */
               value += fr * bil(sino + ((int64_t)b * n_views + a) * W * H, W, H, dX - 0.5,
                                 dY - 0.5, q);
             }
-            if (found) acc_all += value * 2 * REF_PI / blocks; /* :177 */
+            if (found) acc_all += value * 2 * REF_PI / blocks; /* :43 */
           }
           Vb[((int64_t)k * Y + y) * X + x] = acc_all;
         }

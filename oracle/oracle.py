@@ -134,7 +134,7 @@ def standard_geometry(angles_deg, volume_size, detector_size, sid, sdd) -> Geome
 
 def vector_geometry(project_vector, volume_size, detector_size) -> Geometry:
     """The Beijing layer's conventions (Beijing/plug/kernel/forwardKernel.cu:
-    24-35,63-73; backwardKernel.cu:163-177): world = voxel units, step 1,
+    24-35,63-73; backwardKernel.cu:29-43): world = voxel units, step 1,
     scale 1, pixel centres at +1/2, weight SDD/L * 2*pi/(N//21)."""
     pv = _c64(project_vector).reshape(-1, 12)
     n = pv.shape[0]
