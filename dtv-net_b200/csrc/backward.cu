@@ -32,7 +32,10 @@ struct BPMaps {
   float m[kBPParamViews][12];
 };
 static_assert(sizeof(BPMaps) <= 31 * 1024, "kernel parameter space");
-constexpr int kZC = 8;       // voxels per thread along z
+// voxels per thread along z: 8, or 4 / 2 where a volume has too few columns
+// to fill the GPU (bp_zc); the results do not depend on it
+constexpr int kZCMax = 8;
+constexpr int64_t kBPWantBlocks = 4 * 148;  // four resident blocks per SM
 constexpr int kBPThreads = kBPTile * kBPTile;
 
 struct SoftBil {
@@ -66,9 +69,9 @@ struct TableMaps {
   __device__ __forceinline__ const float* row(int jn) const { return v[jn].m; }
 };
 
-// One block's columns: tile `tile` of 16x16 (x, y) columns, z-chunk `zc` of kZC
+// One block's columns: tile `tile` of 16x16 (x, y) columns, z-chunk `zc` of ZC
 // voxels, views n0 .. n0 + n_chunk - 1.
-template <bool kTex, bool kZAff, class Maps>
+template <bool kTex, bool kZAff, int ZC, class Maps>
 __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps, int n0, int n_chunk,
                                            const float* __restrict__ spad, cudaTextureObject_t tex,
                                            float* __restrict__ out, int accumulate, int tile,
@@ -76,11 +79,11 @@ __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps,
   const int tiles_x = (bp.nx + kBPTile - 1) / kBPTile;
   const int i = (tile % tiles_x) * kBPTile + (threadIdx.x & 15);
   const int j = (tile / tiles_x) * kBPTile + (threadIdx.x >> 4);
-  const int k0 = zc * kZC;
+  const int k0 = zc * ZC;
   if (i >= bp.nx || j >= bp.ny) return;
-  float acc[kZC];
+  float acc[ZC];
 #pragma unroll
-  for (int z = 0; z < kZC; ++z) acc[z] = 0.f;
+  for (int z = 0; z < ZC; ++z) acc[z] = 0.f;
   const float fi = (float)i, fj = (float)j;
   const int pu = bp.nu + 2 * kPad;
   const float mu = (float)bp.nu, mv = (float)bp.nv;
@@ -96,15 +99,16 @@ __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps,
     SoftBil smp{spad + (int64_t)n * bp.sino_pad_elems, pu, mu, mv};
     if constexpr (kZAff) {
       const float rh = __frcp_rn(bh);
-      const float u = bu * rh, v0 = fmaf(m6, (float)k0, bv) * rh, dv = m6 * rh;
+      // v from the absolute slice index: the same bits for every z-chunking
+      const float u = bu * rh, vb = bv * rh, dv = m6 * rh;
       float wgt = bp.scale;
       if (bp.power == 2) wgt *= rh * rh;
       else if (bp.power == 1) wgt *= rh;
       const bool col_out = bp.extent && (u + 0.5f < -1.f || u + 0.5f > bp.nx + 1.f);
       if (col_out) continue;
 #pragma unroll
-      for (int z = 0; z < kZC; ++z) {
-        const float v = fmaf((float)z, dv, v0);
+      for (int z = 0; z < ZC; ++z) {
+        const float v = fmaf((float)(k0 + z), dv, vb);
         float wz = wgt;
         if (bp.extent && (v + 0.5f < -1.f || v + 0.5f > bp.ny + 1.f)) wz = 0.f;
         float val;
@@ -114,7 +118,7 @@ __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps,
       }
     } else {
 #pragma unroll
-      for (int z = 0; z < kZC; ++z) {
+      for (int z = 0; z < ZC; ++z) {
         const float fk = (float)(k0 + z);
         const float h = fmaf(m10, fk, bh);
         const float rh = __frcp_rn(h);
@@ -137,7 +141,7 @@ __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps,
   const int64_t plane = (int64_t)bp.nx * bp.ny;
   float* o = out + (int64_t)j * bp.nx + i;
 #pragma unroll
-  for (int z = 0; z < kZC; ++z) {
+  for (int z = 0; z < ZC; ++z) {
     const int k = k0 + z;
     if (k < bp.nz) {
       if (accumulate) o[k * plane] += acc[z];
@@ -146,14 +150,14 @@ __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps,
   }
 }
 
-template <bool kTex, bool kZAff>
+template <bool kTex, bool kZAff, int ZC>
 __global__ void __launch_bounds__(kBPThreads) bp_kernel(BPParams bp, const __grid_constant__ BPMaps maps,
                                                         int n0, int n_chunk,
                                                         const float* __restrict__ spad,
                                                         cudaTextureObject_t tex,
                                                         float* __restrict__ out, int accumulate) {
-  bp_columns<kTex, kZAff>(bp, ParamMaps{&maps}, n0, n_chunk, spad, tex, out, accumulate,
-                          (int)blockIdx.x, (int)blockIdx.y);
+  bp_columns<kTex, kZAff, ZC>(bp, ParamMaps{&maps}, n0, n_chunk, spad, tex, out, accumulate,
+                              (int)blockIdx.x, (int)blockIdx.y);
 }
 
 __global__ void stage_sino_pad_kernel(const float* __restrict__ in, float* __restrict__ out, int nu,
@@ -170,6 +174,36 @@ __global__ void stage_sino_pad_kernel(const float* __restrict__ in, float* __res
   }
 }
 
+// Voxels per thread along z: the largest of 8, 4, 2 whose grid has
+// kBPWantBlocks blocks (2 if none has).
+template <class BlocksFor>
+static int bp_zc(BlocksFor blocks_for) {
+  for (int c = kZCMax; c > 2; c /= 2)
+    if (blocks_for(c) >= kBPWantBlocks) return c;
+  return 2;
+}
+
+template <bool kTex, bool kZAff>
+static void launch_bp_zc(int zc, dim3 grid, cudaStream_t st, const BPParams& bp,
+                         const BPMaps& maps, int n0, int cnt, const float* sp,
+                         cudaTextureObject_t tx, float* ob, int acc) {
+  if (zc == 8)
+    bp_kernel<kTex, kZAff, 8><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, ob, acc);
+  else if (zc == 4)
+    bp_kernel<kTex, kZAff, 4><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, ob, acc);
+  else
+    bp_kernel<kTex, kZAff, 2><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, ob, acc);
+}
+
+static void launch_bp(bool tex, bool zaff, int zc, dim3 grid, cudaStream_t st, const BPParams& bp,
+                      const BPMaps& maps, int n0, int cnt, const float* sp, cudaTextureObject_t tx,
+                      float* ob, int acc) {
+  if (tex && zaff) launch_bp_zc<true, true>(zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
+  else if (tex) launch_bp_zc<true, false>(zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
+  else if (zaff) launch_bp_zc<false, true>(zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
+  else launch_bp_zc<false, false>(zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
+}
+
 int backward_impl(Plan* p, const float* sino, int batch, float* out, int accumulate,
                   cudaStream_t st) {
   const GeomParams& gp = p->gp;
@@ -182,7 +216,8 @@ int backward_impl(Plan* p, const float* sino, int batch, float* out, int accumul
   bp.sino_pad_elems = (int64_t)(gp.nu + 2 * kPad) * (gp.nv + 2 * kPad);
   const bool tex = p->sino_tex != nullptr;  // allocated for the texture plans
   const int tiles = ((gp.nx + kBPTile - 1) / kBPTile) * ((gp.ny + kBPTile - 1) / kBPTile);
-  dim3 grid(tiles, (gp.nz + kZC - 1) / kZC);
+  const int zc = bp_zc([&](int c) { return (int64_t)tiles * ((gp.nz + c - 1) / c); });
+  dim3 grid(tiles, (gp.nz + zc - 1) / zc);
   const int64_t per_item = (int64_t)gp.nu * gp.nv * gp.n_views;
   BPMaps maps;
   for (int b = 0; b < batch; ++b) {
@@ -208,15 +243,7 @@ int backward_impl(Plan* p, const float* sino, int batch, float* out, int accumul
       const int cnt = std::min(kBPParamViews, gp.n_views - n0);
       for (int j = 0; j < cnt; ++j) memcpy(maps.m[j], p->h_bpv[n0 + j].m, sizeof(maps.m[j]));
       const int acc = n0 > 0 ? 1 : accumulate;
-      if (tex && p->bp_zaffine) {
-        bp_kernel<true, true><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, ob, acc);
-      } else if (tex) {
-        bp_kernel<true, false><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, ob, acc);
-      } else if (p->bp_zaffine) {
-        bp_kernel<false, true><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, ob, acc);
-      } else {
-        bp_kernel<false, false><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, ob, acc);
-      }
+      launch_bp(tex, p->bp_zaffine != 0, zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
       note_launch();
       DTV_LAUNCH_CHECK();
     }
@@ -244,6 +271,7 @@ struct BPMany {
 };
 static_assert(sizeof(BPMany) <= 31 * 1024, "kernel parameter space");
 
+template <int ZC>
 __global__ void __launch_bounds__(kBPThreads) bp_many_kernel(const __grid_constant__ BPMany m,
                                                              int accumulate) {
   int k = 0;
@@ -252,11 +280,11 @@ __global__ void __launch_bounds__(kBPThreads) bp_many_kernel(const __grid_consta
   const int local = (int)blockIdx.x - it.block0;
   const int tile = local % it.tiles, zc = local / it.tiles;
   if (it.zaffine)
-    bp_columns<true, true>(it.bp, TableMaps{it.views}, 0, it.bp.n_views, nullptr, it.tex, it.out,
-                           accumulate, tile, zc);
+    bp_columns<true, true, ZC>(it.bp, TableMaps{it.views}, 0, it.bp.n_views, nullptr, it.tex,
+                               it.out, accumulate, tile, zc);
   else
-    bp_columns<true, false>(it.bp, TableMaps{it.views}, 0, it.bp.n_views, nullptr, it.tex, it.out,
-                            accumulate, tile, zc);
+    bp_columns<true, false, ZC>(it.bp, TableMaps{it.views}, 0, it.bp.n_views, nullptr, it.tex,
+                                it.out, accumulate, tile, zc);
 }
 
 int backward_many_impl(Plan* const* plans, const float* const* sinos, float* const* outs, int count,
@@ -264,6 +292,16 @@ int backward_many_impl(Plan* const* plans, const float* const* sinos, float* con
   BPMany m;
   for (int c0 = 0; c0 < count; c0 += kManyItems) {
     const int cnt = std::min(kManyItems, count - c0);
+    // one z-chunk length for the whole launch, from its total column tiles
+    const int zc = bp_zc([&](int c) {
+      int64_t b = 0;
+      for (int k = 0; k < cnt; ++k) {
+        const GeomParams& gp = plans[c0 + k]->gp;
+        b += (int64_t)((gp.nx + kBPTile - 1) / kBPTile) * ((gp.ny + kBPTile - 1) / kBPTile) *
+             ((gp.nz + c - 1) / c);
+      }
+      return b;
+    });
     int64_t blocks = 0;
     for (int k = 0; k < cnt; ++k) {
       Plan* p = plans[c0 + k];
@@ -288,11 +326,13 @@ int backward_many_impl(Plan* const* plans, const float* const* sinos, float* con
       it.tiles = ((gp.nx + kBPTile - 1) / kBPTile) * ((gp.ny + kBPTile - 1) / kBPTile);
       it.block0 = (int)blocks;
       it.zaffine = p->bp_zaffine;
-      blocks += (int64_t)it.tiles * ((gp.nz + kZC - 1) / kZC);
+      blocks += (int64_t)it.tiles * ((gp.nz + zc - 1) / zc);
     }
     DTV_CHECK(blocks < 2147483647LL, "too many blocks for one launch");
     m.count = cnt;
-    bp_many_kernel<<<(unsigned)blocks, kBPThreads, 0, st>>>(m, accumulate);
+    if (zc == 8) bp_many_kernel<8><<<(unsigned)blocks, kBPThreads, 0, st>>>(m, accumulate);
+    else if (zc == 4) bp_many_kernel<4><<<(unsigned)blocks, kBPThreads, 0, st>>>(m, accumulate);
+    else bp_many_kernel<2><<<(unsigned)blocks, kBPThreads, 0, st>>>(m, accumulate);
     note_launch();
     DTV_LAUNCH_CHECK();
   }

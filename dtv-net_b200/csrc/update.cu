@@ -7,7 +7,8 @@
 // size[1]; z: i < N - X*Y). The stencils below apply those matrices and their
 // transposes without building them. Volume kernels run on a (x, y, z-slab)
 // grid: a warp is 32 consecutive x of one row, and each thread marches
-// kZS slices along z, carrying the z-neighbour from one slice to the next.
+// up to kZS slices along z (fewer on small volumes, so the grid fills the
+// GPU), carrying the z-neighbour from one slice to the next.
 //
 // The L1-ball projection (model/PDHG/Utils/L1ball.py:4-17) needs the threshold
 // lambda solving sum_i max(a_i - lambda, 0) = r. The reference Newton-iterates
@@ -49,17 +50,26 @@ struct Dims {
   int X, Y, Z;
   int64_t N;  // X*Y*Z
   int quirk;
+  int zs;  // slices per thread, 1 .. kZS
 };
 
-static Dims make_dims(const int32_t s[3], int quirk) {
+constexpr int kTX = 32, kTY = 8, kZS = 8;  // block 32 x 8 threads, up to 8 slices per thread
+// Blocks a launch should have: four resident blocks of 256 threads on each of
+// the 148 SMs. Small volumes take fewer slices per thread to get there.
+constexpr int64_t kWantBlocks = 4 * 148;
+
+static Dims make_dims(const int32_t s[3], int quirk, int batch) {
   Dims d;
   d.X = s[0]; d.Y = s[1]; d.Z = s[2];
   d.N = (int64_t)s[0] * s[1] * s[2];
   d.quirk = quirk;
+  const int64_t cols = (int64_t)((d.X + kTX - 1) / kTX) * ((d.Y + kTY - 1) / kTY);
+  d.zs = kZS;
+  while (d.zs > 1 && cols * ((d.Z + d.zs - 1) / d.zs) * batch < kWantBlocks &&
+         (int64_t)((d.Z + d.zs / 2 - 1) / (d.zs / 2)) * batch <= 65535)
+    d.zs /= 2;
   return d;
 }
-
-constexpr int kTX = 32, kTY = 8, kZS = 8;  // block 32 x 8 threads, 8 slices per thread
 
 static int check_dims(const int32_t s[3], int batch) {
   DTV_CHECK(s != nullptr, "NULL size");
@@ -73,11 +83,11 @@ static int check_dims(const int32_t s[3], int batch) {
 }
 
 static dim3 grid3(const Dims& d, int batch) {
-  return dim3((d.X + kTX - 1) / kTX, (d.Y + kTY - 1) / kTY, ((d.Z + kZS - 1) / kZS) * batch);
+  return dim3((d.X + kTX - 1) / kTX, (d.Y + kTY - 1) / kTY, ((d.Z + d.zs - 1) / d.zs) * batch);
 }
 static const dim3 kBlock3(kTX, kTY);
 
-// Position of this thread: column (x, y) of batch item b, slices [z0, z0+kZS).
+// Position of this thread: column (x, y) of batch item b, slices [z0, z0+zs).
 struct Col {
   int x, y, z0, nz;  // nz = slices this thread handles
   int64_t base;      // b * N
@@ -87,11 +97,11 @@ __device__ __forceinline__ Col col3(const Dims& d) {
   Col c;
   c.x = blockIdx.x * kTX + threadIdx.x;
   c.y = blockIdx.y * kTY + threadIdx.y;
-  const int zslabs = (d.Z + kZS - 1) / kZS;
+  const int zslabs = (d.Z + d.zs - 1) / d.zs;
   const int zb = blockIdx.z % zslabs;
   const int b = blockIdx.z / zslabs;
-  c.z0 = zb * kZS;
-  c.nz = min(kZS, d.Z - c.z0);
+  c.z0 = zb * d.zs;
+  c.nz = min(d.zs, d.Z - c.z0);
   c.base = (int64_t)b * d.N;
   c.in = c.x < d.X && c.y < d.Y;
   return c;
@@ -133,6 +143,20 @@ __device__ __forceinline__ void decompose(const Dims& d, int64_t i, int& x, int&
   z = (int)zz;
   y = (int)yy;
   x = (int)(r - yy * (unsigned int)d.X);
+}
+
+// (x, y, z) of row j = i - axis_off(d, a), the row whose +1 entry lands on
+// column i of voxel (x, y, z): a step back along axis a, except that the
+// quirk's y offset wraps across rows and slices.
+__device__ __forceinline__ void prev_row(const Dims& d, int a, int64_t j, int x, int y, int z,
+                                         int& xj, int& yj, int& zj) {
+  xj = x;
+  yj = y;
+  zj = z;
+  if (a == 0) xj = x - 1;
+  else if (a == 2) zj = z - 1;
+  else if (!d.quirk) yj = y - 1;
+  else decompose(d, j, xj, yj, zj);
 }
 
 // ---- warp / block reductions ------------------------------------------------------------
@@ -741,7 +765,7 @@ __global__ void __launch_bounds__(256) dtvfista_update_kernel(float* __restrict_
       if (col_valid(d, a, i, c.x, c.y, zz)) {
         const int64_t j = i - axis_off(d, a);
         int xj, yj, zj;
-        decompose(d, j, xj, yj, zj);
+        prev_row(d, a, j, c.x, c.y, zz, xj, yj, zj);
         dt += thr(dfwd(zb, d, a, j, xj, yj, zj));
       }
       fn = fmaf(ts[a], dt, fn);
@@ -792,7 +816,7 @@ __global__ void __launch_bounds__(256) tv_descent_kernel(const float* __restrict
       if (col_valid(d, a, i, c.x, c.y, z)) {
         const int64_t j = i - axis_off(d, a);
         int xj, yj, zj;
-        decompose(d, j, xj, yj, zj);
+        prev_row(d, a, j, c.x, c.y, z, xj, yj, zj);
         float gj[3];
         grad3(fb, d, j, xj, yj, zj, gj);
         const float nj = sqrtf(gj[0] * gj[0] + gj[1] * gj[1] + gj[2] * gj[2]) + 1.f;
@@ -820,7 +844,7 @@ int dtv_diff(const float* f, float* out, const int32_t size[3], int32_t batch, i
   int rc = check_dims(size, batch);
   if (rc) return rc;
   DTV_CHECK(axis >= 0 && axis <= 2, "axis must be 0, 1 or 2");
-  Dims d = make_dims(size, quirk);
+  Dims d = make_dims(size, quirk, batch);
   diff_kernel<<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(f, out, d, axis, transpose); note_launch();
   DTV_LAUNCH_CHECK();
   return DTV_OK;
@@ -832,7 +856,7 @@ int dtv_diff_abs_sums(const void* f, int32_t dt, const int32_t size[3], int32_t 
   DTV_CHECK(dt == DTV_F32 || dt == DTV_F16, "dtype must be f32 or f16");
   int rc = check_dims(size, batch);
   if (rc) return rc;
-  Dims d = make_dims(size, quirk);
+  Dims d = make_dims(size, quirk, batch);
   if (dt == DTV_F32) {
     diff_abs_sums_kernel<float><<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(
         (const float*)f, d, sums); note_launch();
@@ -875,7 +899,7 @@ int dtv_pdhg_dual(const void* fbar, float* p, float* q, float* s, float* c, cons
             "f_dtype must be f32, f16 or bf16");
   int rc = check_dims(size, batch);
   if (rc) return rc;
-  Dims d = make_dims(size, prm->quirk);
+  Dims d = make_dims(size, prm->quirk, batch);
   const int64_t total = d.N * batch;
   DTV_CHECK(total <= 2147483647LL, "volume x batch exceeds 2^31-1 elements");
   cudaStream_t st = as_stream(stream);
@@ -929,7 +953,7 @@ int dtv_pdhg_primal(float* f, void* fbar, const float* recon, float* p, float* q
             "f_dtype must be f32, f16 or bf16");
   int rc = check_dims(size, batch);
   if (rc) return rc;
-  Dims d = make_dims(size, prm->quirk);
+  Dims d = make_dims(size, prm->quirk, batch);
   const L1Chan* ch = reinterpret_cast<const L1Chan*>(ws);
   if (prm->f_dtype == DTV_F32) {
     pdhg_primal_kernel<float><<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(
@@ -992,7 +1016,7 @@ int dtv_dtvfista_maxes(const float* z, const int32_t size[3], int32_t batch, con
   DTV_CHECK(z && size && v && maxes, "NULL argument");
   int rc = check_dims(size, batch);
   if (rc) return rc;
-  Dims d = make_dims(size, 1);
+  Dims d = make_dims(size, 1, batch);
   cudaStream_t st = as_stream(stream);
   // the three max bit patterns live in maxes[0..2] during the reduction
   unsigned int* bits = reinterpret_cast<unsigned int*>(maxes);
@@ -1010,7 +1034,7 @@ int dtv_dtvfista_update(float* f, const float* z, const int32_t size[3], int32_t
   DTV_CHECK(!quirk || maxes, "quirk mode needs maxes");
   int rc = check_dims(size, batch);
   if (rc) return rc;
-  Dims d = make_dims(size, quirk);
+  Dims d = make_dims(size, quirk, batch);
   dtvfista_update_kernel<<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(
       f, z, d, v[0], v[1], v[2], t[0], t[1], t[2], momentum, quirk, maxes); note_launch();
   DTV_LAUNCH_CHECK();
@@ -1030,7 +1054,7 @@ int dtv_tv_descent(const float* f_in, float* f_out, const int32_t size[3], int32
   DTV_CHECK(f_in != f_out, "f_in and f_out must differ");
   int rc = check_dims(size, batch);
   if (rc) return rc;
-  Dims d = make_dims(size, quirk);
+  Dims d = make_dims(size, quirk, batch);
   tv_descent_kernel<<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(f_in, f_out, d, davg); note_launch();
   DTV_LAUNCH_CHECK();
   return DTV_OK;
