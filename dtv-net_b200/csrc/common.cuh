@@ -132,6 +132,7 @@ struct Plan {
   cudaSurfaceObject_t* pair_surf;
   cudaTextureObject_t* pair_tex_dev;
   int fp_ray_tile;           // DTV_TUNE_FP_RAY_TILE
+  int fp_band;               // DTV_TUNE_FP_BAND
   // shared-memory staged forward projector (DTV_PLAN_TMA): the z pairs as a
   // linear [batch][nz+3][ny][pair_pitch] u32 array and its two tensor maps
   // (boxes for chunks along x and along y)
@@ -150,6 +151,10 @@ struct Plan {
 };
 
 constexpr int kNumRayTiles = 8;  // forward-projector ray tiles (DTV_TUNE_FP_RAY_TILE)
+// default forward block order (DTV_TUNE_FP_BAND): bands of kDefaultBand tile
+// rows for staged volumes above kBandAboveBytes, view by view below
+constexpr int kDefaultBand = 4;
+constexpr double kBandAboveBytes = 32.0 * (1 << 20);
 constexpr int kPad = 2;  // zero border of the staged volume
 
 // kernels entry points used across units

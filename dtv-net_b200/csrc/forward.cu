@@ -84,10 +84,33 @@ struct TexSampler {
 static const int kRayTiles[kNumRayTiles][3] = {{4, 4, 3}, {4, 4, 4}, {5, 3, 5}, {4, 4, 2},
                                                {5, 3, 3}, {3, 5, 3}, {6, 2, 5}, {3, 5, 2}};
 
-__device__ __forceinline__ void tile_pixel(const RayParams& rp, int& u, int& v) {
+// The (ray tile, view) of this block of a (tiles, views) grid. View-major:
+// the grid's own order. Band-major (rp.band tile rows per band): blocks in
+// launch order take every view of one band of tiles before the next band, so
+// the blocks resident at any time sample one slab of the volume.
+__device__ __forceinline__ void block_tile_view(const RayParams& rp, int& tile, int& n) {
+  if (rp.band <= 0) {
+    tile = (int)blockIdx.x;
+    n = (int)blockIdx.y;
+    return;
+  }
+  const int tiles = (int)gridDim.x;
+  const int tiles_u = (rp.nu + (1 << rp.ltu) - 1) >> rp.ltu;
+  const int64_t per_band = (int64_t)tiles_u * rp.band;
+  const int64_t lin = (int64_t)blockIdx.y * tiles + blockIdx.x;
+  const int64_t band = lin / (per_band * rp.n_views);
+  const int64_t r = lin - band * per_band * rp.n_views;
+  const int64_t in_band = min(per_band, (int64_t)tiles - band * per_band);  // last band: shorter
+  n = (int)(r / in_band);
+  tile = (int)(band * per_band + (r - (int64_t)n * in_band));
+}
+
+__device__ __forceinline__ void tile_pixel(const RayParams& rp, int& u, int& v, int& n) {
   const int t = threadIdx.x, w = t >> 5, l = t & 31;
   const int tiles_u = (rp.nu + (1 << rp.ltu) - 1) >> rp.ltu;
-  const int tu = blockIdx.x % tiles_u, tv = blockIdx.x / tiles_u;
+  int tile;
+  block_tile_view(rp, tile, n);
+  const int tu = tile % tiles_u, tv = tile / tiles_u;
   const int lwpr = rp.ltu - rp.lwu;  // log2 warps per tile row
   u = (tu << rp.ltu) + ((w & ((1 << lwpr) - 1)) << rp.lwu) + (l & ((1 << rp.lwu) - 1));
   v = (tv << rp.ltv) + ((w >> lwpr) << (5 - rp.lwu)) + (l >> rp.lwu);
@@ -97,9 +120,9 @@ template <class T>
 __global__ void __launch_bounds__(kFPThreads) fp_soft_kernel(RayParams rp, const FPView* __restrict__ views,
                                                              const T* __restrict__ vpad,
                                                              int64_t pad_elems, FPOut o) {
-  int u, v;
-  tile_pixel(rp, u, v);
-  const int n = blockIdx.y, b = blockIdx.z;
+  int u, v, n;
+  tile_pixel(rp, u, v, n);
+  const int b = blockIdx.z;
   float res = 0.f;
   const bool live = u < rp.nu && v < rp.nv;
   if (live) {
@@ -118,9 +141,9 @@ __global__ void __launch_bounds__(kFPThreads) fp_soft_kernel(RayParams rp, const
 __global__ void __launch_bounds__(kFPThreads) fp_quad_kernel(RayParams rp, const FPView* __restrict__ views,
                                                              const float4* __restrict__ quads,
                                                              int64_t pad_elems, FPOut o) {
-  int u, v;
-  tile_pixel(rp, u, v);
-  const int n = blockIdx.y, b = blockIdx.z;
+  int u, v, n;
+  tile_pixel(rp, u, v, n);
+  const int b = blockIdx.z;
   float res = 0.f;
   if (u < rp.nu && v < rp.nv) {
     const RaySetup rs = setup_ray(rp, views[n], u, v);
@@ -137,9 +160,9 @@ __global__ void __launch_bounds__(kFPThreads) fp_quad_kernel(RayParams rp, const
 
 __global__ void __launch_bounds__(kFPThreads) fp_tex_kernel(RayParams rp, const FPView* __restrict__ views,
                                                             const cudaTextureObject_t* texs, FPOut o) {
-  int u, v;
-  tile_pixel(rp, u, v);
-  const int n = blockIdx.y, b = blockIdx.z;
+  int u, v, n;
+  tile_pixel(rp, u, v, n);
+  const int b = blockIdx.z;
   float res = 0.f;
   if (u < rp.nu && v < rp.nv) {
     const RaySetup rs = setup_ray(rp, views[n], u, v, 0.5f, 0.5f);
@@ -153,9 +176,9 @@ __global__ void __launch_bounds__(kFPThreads) fp_tex_kernel(RayParams rp, const 
 __global__ void __launch_bounds__(kFPThreads) fp_pair_kernel(RayParams rp, const FPView* __restrict__ views,
                                                              const cudaTextureObject_t* texs,
                                                              FPOut o) {
-  int u, v;
-  tile_pixel(rp, u, v);
-  const int n = blockIdx.y, b = blockIdx.z;
+  int u, v, n;
+  tile_pixel(rp, u, v, n);
+  const int b = blockIdx.z;
   float res = 0.f;
   if (u < rp.nu && v < rp.nv) {
     const RaySetup rs = setup_ray(rp, views[n], u, v, 0.5f, 0.f);
@@ -349,6 +372,7 @@ int forward_impl(Plan* p, const void* vol, int vol_dtype, int batch, float* out,
   rp.ltu = kRayTiles[p->fp_ray_tile][0];
   rp.ltv = kRayTiles[p->fp_ray_tile][1];
   rp.lwu = kRayTiles[p->fp_ray_tile][2];
+  rp.band = p->fp_band;
   FPOut o{out, g, sigma, abs_sum, epilogue};
   const int tiles = ((gp.nu + (1 << rp.ltu) - 1) >> rp.ltu) * ((gp.nv + (1 << rp.ltv) - 1) >> rp.ltv);
   dim3 grid(tiles, gp.n_views, batch);

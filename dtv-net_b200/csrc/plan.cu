@@ -273,6 +273,17 @@ int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Pla
     }
   }
 #undef PLAN_CUDA
+  // forward block order: bands of 4 tile rows across views once the staged
+  // volume is too large to stay in L2 from one view to the next
+  if (!(flags & DTV_PLAN_TMA)) {
+    const double voxels = (double)gp.nx * gp.ny * gp.nz;
+    double staged;
+    if (flags & DTV_PLAN_TEX_PAIRS) staged = (double)gp.nx * gp.ny * (gp.nz + 3) * 4.0;
+    else if (flags & DTV_PLAN_TEX) staged = voxels * (p->stage_dtype == DTV_F16 ? 2.0 : 4.0);
+    else if (p->d_vol_quads) staged = (double)p->pad_elems * 16.0;
+    else staged = (double)p->pad_elems * 2.0;
+    p->fp_band = staged > kBandAboveBytes ? kDefaultBand : 0;
+  }
   *out = p;
   return DTV_OK;
 }
@@ -326,6 +337,11 @@ int dtv_plan_set_tuning(dtv_plan* plan, int32_t key, int32_t value) {
                 kNumRayTiles - 1);
       p->fp_ray_tile = value;
       return DTV_OK;
+    case DTV_TUNE_FP_BAND:
+      DTV_CHECK(!(p->flags & DTV_PLAN_TMA), "DTV_TUNE_FP_BAND does not apply to DTV_PLAN_TMA plans");
+      DTV_CHECK(value >= 0 && value <= 4096, "DTV_TUNE_FP_BAND must be in [0, 4096]");
+      p->fp_band = value;
+      return DTV_OK;
     default:
       return fail(DTV_ERR_INVALID, "unknown tuning key %d", key);
   }
@@ -343,6 +359,9 @@ int dtv_plan_get_tuning(const dtv_plan* plan, int32_t key, int32_t* value) {
       return DTV_OK;
     case DTV_TUNE_ADJOINT:
       *value = p->adjoint_method;
+      return DTV_OK;
+    case DTV_TUNE_FP_BAND:
+      *value = p->fp_band;
       return DTV_OK;
     default:
       return fail(DTV_ERR_INVALID, "unknown tuning key %d", key);

@@ -15,6 +15,7 @@ struct RayParams {
   float scale;
   // ray tile of a block (tu x tv pixels) and of a warp (wu x wv = 32), log2
   int ltu, ltv, lwu;
+  int band;  // tile rows per band of the band-major block order; 0: view-major
 };
 
 inline RayParams make_ray_params(const GeomParams& gp) {
@@ -26,6 +27,7 @@ inline RayParams make_ray_params(const GeomParams& gp) {
   r.step = gp.step;
   r.scale = (float)gp.scale;
   r.ltu = 4; r.ltv = 4; r.lwu = 3;
+  r.band = 0;
   return r;
 }
 

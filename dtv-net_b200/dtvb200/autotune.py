@@ -20,6 +20,11 @@ DTV_TUNE_ADJOINT applies to plans with adjoint tables: the exact adjoint
 scatters either per 16^3 brick through shared-memory atomics (0) or into
 per-cell records with 16-byte vector atomics in L2 (1); which is faster
 depends on whether the records fit in L2. It is timed on plan.adjoint.
+
+DTV_TUNE_FP_BAND picks the forward projector's block order: view by view (0),
+or bands of B tile rows with every view of a band before the next band, which
+keeps the volume slab under a band in L2 across views when the staged volume
+is larger than L2.
 """
 from __future__ import annotations
 
@@ -31,7 +36,7 @@ from .geometry import Plan
 _CACHE: dict = {}
 N_RAY_TILES = 8
 CANDIDATES = {_lib.DTV_TUNE_FP_RAY_TILE: range(N_RAY_TILES), _lib.DTV_TUNE_FP_TEX_SHARE: range(9),
-              _lib.DTV_TUNE_ADJOINT: range(2)}
+              _lib.DTV_TUNE_ADJOINT: range(2), _lib.DTV_TUNE_FP_BAND: (0, 1, 2, 4, 8, 16, 32)}
 
 
 def _key(plan: Plan, batch: int, key: int):

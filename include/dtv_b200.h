@@ -186,6 +186,13 @@ DTV_API int dtv_plan_destroy(dtv_plan* plan);
  *   with 16-byte vector atomics, then a gather (needs DTV_PLAN_ADJOINT; the
  *   default for such plans). No counterpart in the reference. */
 #define DTV_TUNE_ADJOINT 3
+/*   DTV_TUNE_FP_BAND: the order in which the forward projector's ray tiles
+ *   run. 0: view by view. B > 0: bands of B tile rows, every view of a band
+ *   before the next band, so the volume slab a band's rays cross stays in L2
+ *   across views. Default: 4 when the plan's staged volume exceeds 32 MB, else
+ *   0. 0..4096; not used by DTV_PLAN_TMA plans. No counterpart in the
+ *   reference. */
+#define DTV_TUNE_FP_BAND 4
 DTV_API int dtv_plan_set_tuning(dtv_plan* plan, int32_t key, int32_t value);
 DTV_API int dtv_plan_get_tuning(const dtv_plan* plan, int32_t key, int32_t* value);
 /* Device-side error bits of the plan's kernels (0: none; 1: a shared-memory

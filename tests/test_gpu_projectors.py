@@ -148,6 +148,34 @@ def test_forward_ray_tiles_agree(cuda, sampler):
         assert torch.equal(plan.forward(vol), ref), t
 
 
+@pytest.mark.parametrize("sampler", ["soft", "tex", "pairs"])
+def test_forward_band_orders_agree(cuda, sampler):
+    """Every forward block order (view by view, or bands of tile rows across
+    views, with a partial last band) computes the same per-ray sums."""
+    g, og = make_case("standard_odd")
+    plan = dtvb200.Plan(g, max_batch=2, sampler=sampler, device=cuda)
+    vol = to_dev(blob_volume(np.random.default_rng(25), og.vol_shape, 2), cuda)
+    key = _lib.DTV_TUNE_FP_BAND
+    assert plan.get_tuning(key) == 0  # a small staged volume runs view by view
+    ref = plan.forward(vol).clone()
+    for tile in (0, 6, 2):  # 16x16, 64x4 (four tile rows), 32x8 ray tiles
+        plan.set_tuning(_lib.DTV_TUNE_FP_RAY_TILE, tile)
+        for band in (0, 1, 3, 4096):
+            plan.set_tuning(key, band)
+            assert torch.equal(plan.forward(vol), ref), (tile, band)
+    for bad in (-1, 4097):
+        with pytest.raises(dtvb200.DtvError):
+            plan.set_tuning(key, bad)
+    with pytest.raises(dtvb200.DtvError):
+        dtvb200.Plan(g, sampler="tma", device=cuda).set_tuning(key, 1)
+    # a staged volume above 32 MB (FP32 quad records of 128^3) runs in bands
+    big = dtvb200.circular([0.0, 90.0], (128, 128, 128), (1.0,) * 3, (64, 64), (2.0, 2.0), 500, 1000)
+    assert dtvb200.Plan(big, sampler="soft", device=cuda).get_tuning(key) == 4
+    t = dtvb200.autotune.tune(plan, key=key, reps=2, warmup=1, use_cache=False)
+    assert sorted(t) == list(dtvb200.autotune.CANDIDATES[key])
+    assert plan.get_tuning(key) == min(t, key=t.get)
+
+
 def test_tuning_keys_and_autotune(cuda):
     g, og = make_case("standard")
     plan = dtvb200.Plan(g, sampler="pairs", device=cuda)
