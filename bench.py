@@ -43,7 +43,7 @@ TEXTURE_FETCH_PEAK = 1.116e12
 # DRAM traffic of one forward-projector launch on this workload
 # (dram__bytes_read.sum + dram__bytes_write.sum, one ncu --set full capture of
 # `python bench.py --profile 12`) and that capture's texture-pipe utilisation.
-FP_NCU = {"pairs": {"traffic": 275.710976e6 + 61.128192e6, "tex_pipe_pct": 93.7}}
+FP_NCU = {"pairs": {"traffic": 142.958336e6 + 26.171136e6, "tex_pipe_pct": 95.3}}
 
 
 def workload_name(c):

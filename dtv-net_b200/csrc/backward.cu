@@ -22,6 +22,7 @@ struct BPParams {
   int extent;
   float scale;
   int64_t sino_pad_elems;  // one padded view
+  int warp;                // columns of a warp and a quad (DTV_TUNE_BP_WARP)
 };
 
 constexpr int kBPTile = 16;  // columns per block edge
@@ -77,8 +78,34 @@ __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps,
                                            float* __restrict__ out, int accumulate, int tile,
                                            int zc) {
   const int tiles_x = (bp.nx + kBPTile - 1) / kBPTile;
-  const int i = (tile % tiles_x) * kBPTile + (threadIdx.x & 15);
-  const int j = (tile / tiles_x) * kBPTile + (threadIdx.x >> 4);
+  // this thread's column in the 16 x 16 tile; a warp covers 16 x 2, 8 x 4 or
+  // 4 x 8 columns (the narrower, the fewer detector rows' cache sectors one
+  // fetch instruction touches when a voxel spans several pixels)
+  const int t = (int)threadIdx.x;
+  int li, lj;
+  if (bp.warp >= 3) {
+    // quads (4 consecutive lanes) of 2 x 2 columns; a warp of 8 quads covers
+    // 8 x 4 (warp 3) or 4 x 8 (warp 4) columns
+    const int q = (t >> 2) & 7, qi = t & 1, qj = (t >> 1) & 1, w = t >> 5;
+    if (bp.warp == 3) {
+      li = ((q & 3) << 1 | qi) | ((w & 1) << 3);
+      lj = ((q >> 2) << 1 | qj) | ((w >> 1) << 2);
+    } else {
+      li = ((q & 1) << 1 | qi) | ((w & 3) << 2);
+      lj = ((q >> 1) << 1 | qj) | ((w >> 2) << 3);
+    }
+  } else if (bp.warp == 1) {
+    li = (t & 7) | (((t >> 5) & 1) << 3);
+    lj = ((t >> 3) & 3) | ((t >> 6) << 2);
+  } else if (bp.warp == 2) {
+    li = (t & 3) | (((t >> 5) & 3) << 2);
+    lj = ((t >> 2) & 7) | ((t >> 7) << 3);
+  } else {
+    li = t & 15;
+    lj = t >> 4;
+  }
+  const int i = (tile % tiles_x) * kBPTile + li;
+  const int j = (tile / tiles_x) * kBPTile + lj;
   const int k0 = zc * ZC;
   if (i >= bp.nx || j >= bp.ny) return;
   float acc[ZC];
@@ -214,6 +241,7 @@ int backward_impl(Plan* p, const float* sino, int batch, float* out, int accumul
   bp.extent = gp.bp_extent;
   bp.scale = (float)gp.bp_scale;
   bp.sino_pad_elems = (int64_t)(gp.nu + 2 * kPad) * (gp.nv + 2 * kPad);
+  bp.warp = p->bp_warp;
   const bool tex = p->sino_tex != nullptr;  // allocated for the texture plans
   const int tiles = ((gp.nx + kBPTile - 1) / kBPTile) * ((gp.ny + kBPTile - 1) / kBPTile);
   const int zc = bp_zc([&](int c) { return (int64_t)tiles * ((gp.nz + c - 1) / c); });
@@ -320,6 +348,7 @@ int backward_many_impl(Plan* const* plans, const float* const* sinos, float* con
       it.bp.extent = gp.bp_extent;
       it.bp.scale = (float)gp.bp_scale;
       it.bp.sino_pad_elems = 0;
+      it.bp.warp = p->bp_warp;
       it.views = p->d_bpv;
       it.tex = p->sino_tex[0];
       it.out = outs[c0 + k];

@@ -133,6 +133,7 @@ struct Plan {
   cudaTextureObject_t* pair_tex_dev;
   int fp_ray_tile;           // DTV_TUNE_FP_RAY_TILE
   int fp_band;               // DTV_TUNE_FP_BAND
+  int bp_warp;               // DTV_TUNE_BP_WARP
   // shared-memory staged forward projector (DTV_PLAN_TMA): the z pairs as a
   // linear [batch][nz+3][ny][pair_pitch] u32 array and its two tensor maps
   // (boxes for chunks along x and along y)

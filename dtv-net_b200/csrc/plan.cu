@@ -273,6 +273,7 @@ int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Pla
     }
   }
 #undef PLAN_CUDA
+  p->bp_warp = 4;  // 4 x 8 columns per warp in quads of 2 x 2 (fewest texture wavefronts)
   // forward block order: bands of 4 tile rows across views once the staged
   // volume is too large to stay in L2 from one view to the next
   if (!(flags & DTV_PLAN_TMA)) {
@@ -342,6 +343,10 @@ int dtv_plan_set_tuning(dtv_plan* plan, int32_t key, int32_t value) {
       DTV_CHECK(value >= 0 && value <= 4096, "DTV_TUNE_FP_BAND must be in [0, 4096]");
       p->fp_band = value;
       return DTV_OK;
+    case DTV_TUNE_BP_WARP:
+      DTV_CHECK(value >= 0 && value <= 4, "DTV_TUNE_BP_WARP must be in [0, 4]");
+      p->bp_warp = value;
+      return DTV_OK;
     default:
       return fail(DTV_ERR_INVALID, "unknown tuning key %d", key);
   }
@@ -362,6 +367,9 @@ int dtv_plan_get_tuning(const dtv_plan* plan, int32_t key, int32_t* value) {
       return DTV_OK;
     case DTV_TUNE_FP_BAND:
       *value = p->fp_band;
+      return DTV_OK;
+    case DTV_TUNE_BP_WARP:
+      *value = p->bp_warp;
       return DTV_OK;
     default:
       return fail(DTV_ERR_INVALID, "unknown tuning key %d", key);

@@ -21,6 +21,7 @@ DTV_TUNE_FP_RAY_TILE = 1
 DTV_TUNE_FP_TEX_SHARE = 2
 DTV_TUNE_ADJOINT = 3
 DTV_TUNE_FP_BAND = 4
+DTV_TUNE_BP_WARP = 5
 DTV_EPI_STORE, DTV_EPI_RESIDUAL, DTV_EPI_PDHG = 0, 1, 2
 
 

@@ -25,6 +25,9 @@ DTV_TUNE_FP_BAND picks the forward projector's block order: view by view (0),
 or bands of B tile rows with every view of a band before the next band, which
 keeps the volume slab under a band in L2 across views when the staged volume
 is larger than L2.
+
+DTV_TUNE_BP_WARP picks the backprojector's columns per warp (16 x 2, 8 x 4 or
+4 x 8). It is timed on plan.backward.
 """
 from __future__ import annotations
 
@@ -36,7 +39,8 @@ from .geometry import Plan
 _CACHE: dict = {}
 N_RAY_TILES = 8
 CANDIDATES = {_lib.DTV_TUNE_FP_RAY_TILE: range(N_RAY_TILES), _lib.DTV_TUNE_FP_TEX_SHARE: range(9),
-              _lib.DTV_TUNE_ADJOINT: range(2), _lib.DTV_TUNE_FP_BAND: (0, 1, 2, 4, 8, 16, 32)}
+              _lib.DTV_TUNE_ADJOINT: range(2), _lib.DTV_TUNE_FP_BAND: (0, 1, 2, 4, 8, 16, 32),
+              _lib.DTV_TUNE_BP_WARP: range(5)}
 
 
 def _key(plan: Plan, batch: int, key: int):
@@ -89,6 +93,8 @@ def tune(plan: Plan, batch: int = 1, key: int = None, candidates=None,
     sino = torch.rand(plan.sino_shape(batch), device=plan.device, generator=gen)
     if key == _lib.DTV_TUNE_ADJOINT:
         fn = lambda: plan.adjoint(sino, vol)  # noqa: E731
+    elif key == _lib.DTV_TUNE_BP_WARP:
+        fn = lambda: plan.backward(sino, vol)  # noqa: E731
     else:
         fn = lambda: plan.forward(vol, sino)  # noqa: E731
     times = {}

@@ -193,6 +193,12 @@ DTV_API int dtv_plan_destroy(dtv_plan* plan);
  *   0. 0..4096; not used by DTV_PLAN_TMA plans. No counterpart in the
  *   reference. */
 #define DTV_TUNE_FP_BAND 4
+/*   DTV_TUNE_BP_WARP: the backprojector's columns per warp and per quad of
+ *   4 consecutive lanes: 0 = 16 x 2 (quads 4 x 1), 1 = 8 x 4 (4 x 1),
+ *   2 = 4 x 8 (4 x 1), 3 = 8 x 4 (2 x 2), 4 = 4 x 8 (2 x 2, default). The
+ *   texture unit serves a quad in fewer wavefronts when its four footprints
+ *   are close. No counterpart in the reference. */
+#define DTV_TUNE_BP_WARP 5
 DTV_API int dtv_plan_set_tuning(dtv_plan* plan, int32_t key, int32_t value);
 DTV_API int dtv_plan_get_tuning(const dtv_plan* plan, int32_t key, int32_t* value);
 /* Device-side error bits of the plan's kernels (0: none; 1: a shared-memory

@@ -215,6 +215,27 @@ def test_backward_fdk_matches_oracle(cuda, kind, sampler):
         assert rel_rmse(out, ref) < 5e-4
 
 
+@pytest.mark.parametrize("kind", ["standard_odd", "vector"])
+@pytest.mark.parametrize("sampler", ["soft", "pairs"])
+def test_backward_warp_layouts_agree(cuda, kind, sampler):
+    """Every backprojector warp / quad layout computes the same voxels
+    (z-affine and general maps, software and texture sampling)."""
+    g, og = make_case(kind)
+    plan = dtvb200.Plan(g, max_batch=2, sampler=sampler, device=cuda)
+    key = _lib.DTV_TUNE_BP_WARP
+    assert plan.get_tuning(key) == 4
+    sino = to_dev(np.random.default_rng(26).random((2, 1) + og.sino_shape), cuda)
+    ref = plan.backward(sino).clone()
+    for w in range(5):
+        plan.set_tuning(key, w)
+        assert torch.equal(plan.backward(sino), ref), w
+    for bad in (-1, 5):
+        with pytest.raises(dtvb200.DtvError):
+            plan.set_tuning(key, bad)
+    t = dtvb200.autotune.tune(plan, key=key, reps=2, warmup=1, use_cache=False)
+    assert sorted(t) == list(range(5)) and plan.get_tuning(key) == min(t, key=t.get)
+
+
 def test_backward_accumulate(cuda):
     g, og = make_case("standard")
     plan = dtvb200.Plan(g, device=cuda)
