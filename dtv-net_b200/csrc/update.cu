@@ -53,7 +53,10 @@ struct Dims {
   int zs;  // slices per thread, 1 .. kZS
 };
 
-constexpr int kTX = 32, kTY = 8, kZS = 8;  // block 32 x 8 threads, up to 8 slices per thread
+// block of 64 x 4 threads (each warp 32 consecutive x of one row; a block's
+// rows are 256 contiguous bytes, which streams better than 32 x 8), up to 8
+// slices per thread
+constexpr int kTX = 64, kTY = 4, kZS = 8;
 // Blocks a launch should have: four resident blocks of 256 threads on each of
 // the 148 SMs. Small volumes take fewer slices per thread to get there.
 constexpr int64_t kWantBlocks = 4 * 148;
@@ -543,6 +546,9 @@ __global__ void l1_apply_kernel(const float* __restrict__ v, float* __restrict__
 }
 
 // ---- fused PDHG dual step (DTVCP.py:41-47) + level-1 histograms --------------------------------
+// Slices per thread of the dual step (its duals of all slices are held in
+// registers before any store, so fewer slices mean more resident blocks).
+constexpr int kDualZS = 4;
 template <class T>
 __global__ void __launch_bounds__(256) pdhg_dual_kernel(const T* __restrict__ fbar, float* __restrict__ p,
                                                         float* __restrict__ q, float* __restrict__ s,
@@ -563,9 +569,9 @@ __global__ void __launch_bounds__(256) pdhg_dual_kernel(const T* __restrict__ fb
   // phase 1: the duals of all slices are loaded first (a later slice's loads
   // cannot move above an earlier slice's stores to the same arrays), then
   // stencils and stores
-  float pv[kZS], qv[kZS], sv[kZS], cv[kZS];
+  float pv[kDualZS], qv[kDualZS], sv[kDualZS], cv[kDualZS];
 #pragma unroll
-  for (int k = 0; k < kZS; ++k) {
+  for (int k = 0; k < kDualZS; ++k) {
     pv[k] = qv[k] = sv[k] = cv[k] = 0.f;
     if (cl.in && k < cl.nz) {
       const int64_t t = cl.base + i0 + k * plane;
@@ -575,9 +581,9 @@ __global__ void __launch_bounds__(256) pdhg_dual_kernel(const T* __restrict__ fb
       cv[k] = c[t];
     }
   }
-  unsigned int keys[3][kZS];
+  unsigned int keys[3][kDualZS];
 #pragma unroll
-  for (int k = 0; k < kZS; ++k) {
+  for (int k = 0; k < kDualZS; ++k) {
     keys[0][k] = keys[1][k] = keys[2][k] = 0u;
     if (cl.in && k < cl.nz) {
       const int64_t i = i0 + k * plane;
@@ -600,7 +606,7 @@ __global__ void __launch_bounds__(256) pdhg_dual_kernel(const T* __restrict__ fb
   }
   // phase 2: level-1 histograms (warp-synchronous; every lane takes part)
 #pragma unroll
-  for (int k = 0; k < kZS; ++k) {
+  for (int k = 0; k < kDualZS; ++k) {
     const bool in = cl.in && k < cl.nz;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -907,19 +913,23 @@ int dtv_pdhg_dual(const void* fbar, float* p, float* q, float* s, float* c, cons
   const float sg = prm->sigma;
   // radius on |p_| directly: sigma * v_a * t_a (the reference projects |p_|/sigma
   // onto the ball of radius v_a * t_a)
+  Dims dd = d;
+  dd.zs = std::min(d.zs, kDualZS);
+  DTV_CHECK((int64_t)((d.Z + dd.zs - 1) / dd.zs) * batch <= 65535,
+            "z slabs x batch exceeds the grid limit of the dual step");
   l1_reset_kernel<<<1, 32, 0, st>>>(ch, 3, nullptr, t, sg * prm->v[0], sg * prm->v[1],
                                     sg * prm->v[2]); note_launch();
   if (prm->f_dtype == DTV_F32) {
-    pdhg_dual_kernel<float><<<grid3(d, batch), kBlock3, 0, st>>>(
-        (const float*)fbar, p, q, s, c, d, prm->v[0] * sg, prm->v[1] * sg, prm->v[2] * sg,
+    pdhg_dual_kernel<float><<<grid3(dd, batch), kBlock3, 0, st>>>(
+        (const float*)fbar, p, q, s, c, dd, prm->v[0] * sg, prm->v[1] * sg, prm->v[2] * sg,
         sg * prm->mu, ch); note_launch();
   } else if (prm->f_dtype == DTV_F16) {
-    pdhg_dual_kernel<__half><<<grid3(d, batch), kBlock3, 0, st>>>(
-        (const __half*)fbar, p, q, s, c, d, prm->v[0] * sg, prm->v[1] * sg, prm->v[2] * sg,
+    pdhg_dual_kernel<__half><<<grid3(dd, batch), kBlock3, 0, st>>>(
+        (const __half*)fbar, p, q, s, c, dd, prm->v[0] * sg, prm->v[1] * sg, prm->v[2] * sg,
         sg * prm->mu, ch); note_launch();
   } else {
-    pdhg_dual_kernel<__nv_bfloat16><<<grid3(d, batch), kBlock3, 0, st>>>(
-        (const __nv_bfloat16*)fbar, p, q, s, c, d, prm->v[0] * sg, prm->v[1] * sg,
+    pdhg_dual_kernel<__nv_bfloat16><<<grid3(dd, batch), kBlock3, 0, st>>>(
+        (const __nv_bfloat16*)fbar, p, q, s, c, dd, prm->v[0] * sg, prm->v[1] * sg,
         prm->v[2] * sg, sg * prm->mu, ch); note_launch();
   }
   DTV_LAUNCH_CHECK();

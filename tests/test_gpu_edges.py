@@ -1,6 +1,6 @@
 """GPU parity tests on degenerate and ragged shapes: one voxel, one z-slice,
 a one-voxel column, one detector pixel, one detector row, one view, and sizes
-one past every tile edge of the kernels (32 x 8 update tiles, 16 x 16
+one past every tile edge of the kernels (64 x 4 update tiles, 16 x 16
 projector tiles, 8-slice z runs). Every sampler, the FDK backprojector, both
 exact adjoints and the PDHG / L1-ball updates are compared with the FP64
 oracle on the same inputs.
@@ -154,7 +154,7 @@ def test_edge_adjoint_and_dot_test(cuda, kind, table, method):
     assert abs(lhs - rhs) / abs(lhs) < 1e-5
 
 
-EDGE_VOLS = [(1, 1, 1), (1, 1, 9), (7, 1, 1), (1, 6, 1), (33, 9, 17), (32, 8, 8)]
+EDGE_VOLS = [(1, 1, 1), (1, 1, 9), (7, 1, 1), (1, 6, 1), (33, 9, 17), (32, 8, 8), (65, 5, 9)]
 
 
 @pytest.mark.parametrize("vs", EDGE_VOLS)
