@@ -16,10 +16,12 @@
  *     and dtv_last_error_message() gives the detail of the last failure on the
  *     calling thread (the reference raised RuntimeError via AT_ASSERTM on bad
  *     input, forwardKernel.cu:15-17,89-94, and ignored CUDA errors).
- *   - plans are immutable after creation; a plan may be used from several
- *     host threads on different streams at once EXCEPT that calls sharing one
- *     plan's staging buffers (forward/backward) on different streams race:
- *     serialise them on one stream or use one plan per stream.
+ *   - plans are immutable after creation apart from their launch knobs
+ *     (dtv_plan_set_tuning, which a launch reads when it is issued; set them
+ *     before sharing the plan between threads). A plan may be used from
+ *     several host threads on different streams at once EXCEPT that calls
+ *     sharing one plan's staging buffers (forward/backward) on different
+ *     streams race: serialise them on one stream or use one plan per stream.
  */
 #ifndef DTV_B200_H
 #define DTV_B200_H
