@@ -109,6 +109,24 @@ __device__ __forceinline__ Col col3(const Dims& d) {
   c.in = c.x < d.X && c.y < d.Y;
   return c;
 }
+// The same position for tile `tile` of that grid, in its launch order (x
+// tiles fastest, then y tiles, then z-slabs and batch items).
+__device__ __forceinline__ Col col3_tile(const Dims& d, int64_t tile) {
+  const int tx = (d.X + kTX - 1) / kTX, ty = (d.Y + kTY - 1) / kTY;
+  const int bx = (int)(tile % tx);
+  const int64_t r = tile / tx;
+  const int by = (int)(r % ty);
+  const int bz = (int)(r / ty);
+  const int zslabs = (d.Z + d.zs - 1) / d.zs;
+  Col c;
+  c.x = bx * kTX + threadIdx.x;
+  c.y = by * kTY + threadIdx.y;
+  c.z0 = (bz % zslabs) * d.zs;
+  c.nz = min(d.zs, d.Z - c.z0);
+  c.base = (int64_t)(bz / zslabs) * d.N;
+  c.in = c.x < d.X && c.y < d.Y;
+  return c;
+}
 __device__ __forceinline__ int ltid() { return threadIdx.y * blockDim.x + threadIdx.x; }
 __device__ __forceinline__ int lthreads() { return blockDim.x * blockDim.y; }
 
@@ -550,16 +568,18 @@ __global__ void l1_apply_kernel(const float* __restrict__ v, float* __restrict__
 // registers before any store, so fewer slices mean more resident blocks).
 constexpr int kDualZS = 4;
 template <class T>
-__global__ void __launch_bounds__(256) pdhg_dual_kernel(const T* __restrict__ fbar, float* __restrict__ p,
+__global__ void __launch_bounds__(256, 6) pdhg_dual_kernel(const T* __restrict__ fbar, float* __restrict__ p,
                                                         float* __restrict__ q, float* __restrict__ s,
                                                         float* __restrict__ c, Dims d, float a0,
                                                         float a1, float a2, float smu,
-                                                        L1Chan* chans) {
+                                                        L1Chan* chans, int64_t n_tiles) {
   __shared__ unsigned int hs[3][3 * kL1B1];
   for (int i = ltid(); i < 9 * kL1B1; i += lthreads()) (&hs[0][0])[i] = 0u;
   __syncthreads();
-  const Col cl = col3(d);
   unsigned int kmax[3] = {0u, 0u, 0u};
+  // a block walks several tiles and flushes its histograms once
+  for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+  const Col cl = col3_tile(d, tile);
   const T* fb = fbar + cl.base;
   const int64_t plane = (int64_t)d.X * d.Y;
   const int64_t oy = axis_off(d, 1);
@@ -613,6 +633,7 @@ __global__ void __launch_bounds__(256) pdhg_dual_kernel(const T* __restrict__ fb
       kmax[a] = max(kmax[a], keys[a][k]);
       hist_add(hs[a], kL1B1, (int)(keys[a][k] >> kL1S1), keys[a][k], in);
     }
+  }
   }
   __syncthreads();
 #pragma unroll
@@ -915,22 +936,27 @@ int dtv_pdhg_dual(const void* fbar, float* p, float* q, float* s, float* c, cons
   // onto the ball of radius v_a * t_a)
   Dims dd = d;
   dd.zs = std::min(d.zs, kDualZS);
-  DTV_CHECK((int64_t)((d.Z + dd.zs - 1) / dd.zs) * batch <= 65535,
-            "z slabs x batch exceeds the grid limit of the dual step");
+  // tiles of the (x, y, z-slab) grid, walked by at most six resident blocks
+  // per SM, each adding at most 2^20 elements to its histograms
+  const int64_t tiles = (int64_t)((d.X + kTX - 1) / kTX) * ((d.Y + kTY - 1) / kTY) *
+                        ((d.Z + dd.zs - 1) / dd.zs) * batch;
+  const int64_t per_block = kHistBlockElems / (kTX * kTY * kDualZS);
+  const int grid = (int)std::max<int64_t>(std::min<int64_t>(tiles, 148LL * 6),
+                                          (tiles + per_block - 1) / per_block);
   l1_reset_kernel<<<1, 32, 0, st>>>(ch, 3, nullptr, t, sg * prm->v[0], sg * prm->v[1],
                                     sg * prm->v[2]); note_launch();
   if (prm->f_dtype == DTV_F32) {
-    pdhg_dual_kernel<float><<<grid3(dd, batch), kBlock3, 0, st>>>(
+    pdhg_dual_kernel<float><<<grid, kBlock3, 0, st>>>(
         (const float*)fbar, p, q, s, c, dd, prm->v[0] * sg, prm->v[1] * sg, prm->v[2] * sg,
-        sg * prm->mu, ch); note_launch();
+        sg * prm->mu, ch, tiles); note_launch();
   } else if (prm->f_dtype == DTV_F16) {
-    pdhg_dual_kernel<__half><<<grid3(dd, batch), kBlock3, 0, st>>>(
+    pdhg_dual_kernel<__half><<<grid, kBlock3, 0, st>>>(
         (const __half*)fbar, p, q, s, c, dd, prm->v[0] * sg, prm->v[1] * sg, prm->v[2] * sg,
-        sg * prm->mu, ch); note_launch();
+        sg * prm->mu, ch, tiles); note_launch();
   } else {
-    pdhg_dual_kernel<__nv_bfloat16><<<grid3(dd, batch), kBlock3, 0, st>>>(
+    pdhg_dual_kernel<__nv_bfloat16><<<grid, kBlock3, 0, st>>>(
         (const __nv_bfloat16*)fbar, p, q, s, c, dd, prm->v[0] * sg, prm->v[1] * sg,
-        prm->v[2] * sg, sg * prm->mu, ch); note_launch();
+        prm->v[2] * sg, sg * prm->mu, ch, tiles); note_launch();
   }
   DTV_LAUNCH_CHECK();
   // the shared-memory limit is a per-device function attribute
