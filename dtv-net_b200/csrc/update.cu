@@ -668,15 +668,17 @@ __global__ void __launch_bounds__(256) pdhg_primal_kernel(float* __restrict__ f,
   int64_t i = ((int64_t)cl.z0 * d.Y + cl.y) * d.X + cl.x;
   float sprev = cl.z0 >= 1 ? clipf(sb[i - plane], m2) : 0.f;  // s(i - XY), carried along z
   for (int k = 0; k < cl.nz; ++k, i += plane) {
-    const float ps = clipf(pb[i], m0), qs = clipf(qb[i], m1), ss = clipf(sb[i], m2);
+    const float pr = pb[i], qr = qb[i], sr = sb[i];
+    const float ps = clipf(pr, m0), qs = clipf(qr, m1), ss = clipf(sr, m2);
     float dx = -ps, dy = -qs, dz = -ss;
     if (cl.x >= 1) dx += clipf(pb[i - 1], m0);
     const bool yv = d.quirk ? (i >= d.Y) : (cl.y >= 1);
     if (yv) dy += clipf(qb[i - oy], m1);
     if (cl.z0 + k >= 1) dz += sprev;
-    pb[i] = ps;
-    qb[i] = qs;
-    sb[i] = ss;
+    // only clipped duals change; the others keep their bytes without a store
+    if (ps != pr) pb[i] = ps;
+    if (qs != qr) qb[i] = qs;
+    if (ss != sr) sb[i] = ss;
     sprev = ss;
     const int64_t t = cl.base + i;
     const float reg = fmaf(v0, dx, fmaf(v1, dy, fmaf(v2, dz, mu * c[t])));
