@@ -618,7 +618,9 @@ __global__ void __launch_bounds__(256, 6) pdhg_dual_kernel(const T* __restrict__
       p[t] = np;
       q[t] = nq;
       s[t] = ns;
-      c[t] = fminf(fmaf(smu, fc, cv[k]), 0.f);  // -relu(-c - sigma*mu*fbar)
+      // -relu(-c - sigma*mu*fbar): stays 0 wherever fbar >= 0, stored only on change
+      const float cn = fminf(fmaf(smu, fc, cv[k]), 0.f);
+      if (cn != cv[k]) c[t] = cn;
       keys[0][k] = __float_as_uint(np) & 0x7FFFFFFFu;
       keys[1][k] = __float_as_uint(nq) & 0x7FFFFFFFu;
       keys[2][k] = __float_as_uint(ns) & 0x7FFFFFFFu;
