@@ -740,7 +740,10 @@ def run_large512(args):
 
 def run_profile(args):
     """N eager iterations of the workload (for ncu): forward projector,
-    backprojector and fused updates, one launch each per iteration."""
+    backprojector and fused updates, one launch each per iteration. With
+    --workload large512 the volume is 512^3 and the scan 90 views of 1024x768
+    at 0.8 mm (the sparse subset of that workload); --fp-band overrides the
+    plan's forward block order (DTV_TUNE_FP_BAND)."""
     import torch
 
     import dtvb200
@@ -749,8 +752,12 @@ def run_profile(args):
     c = dict(CFG)
     if args.small:
         c.update(nx=64, ny=64, nz=64, nu=96, nv=96, n_views=16)
+    elif args.workload == "large512":
+        c.update(nx=512, ny=512, nz=512, nu=1024, nv=768, pitch=0.8, n_views=90)
     geo, truth, _ = make_problem(dev, c, c["seed"])
     plan = dtvb200.Plan(geo, max_batch=1, sampler=args.sampler, device=dev)
+    if args.fp_band is not None:
+        plan.set_tuning(dtvb200._lib.DTV_TUNE_FP_BAND, args.fp_band)
     sino = poisson_noise(plan.forward(truth), c["i0"], seed=c["seed"])
     prm = dtv_params(plan, dev)
     alg = dtvb200.DTVCP(plan, args.profile, t_refresh=10, use_graph=False, **prm)
@@ -781,7 +788,11 @@ def main():
                          "FP + BP + 20 FISTA-TV iterations; large512: 512^3 360-view scan + "
                          "50 DTV iterations on 90 views, FP32 and BF16 storage")
     ap.add_argument("--profile", type=int, default=0, metavar="N",
-                    help="profiling run: N eager DTV iterations of the workload, no timing")
+                    help="profiling run: N eager DTV iterations of the workload, no timing "
+                         "(sparse_dtv, or large512's 90-view subset)")
+    ap.add_argument("--fp-band", type=int, default=None, metavar="B",
+                    help="profiling run: forward block order (0: view by view; B: bands of "
+                         "B tile rows)")
     args = ap.parse_args()
     if args.warmup < 3 and not args.small:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
