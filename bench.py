@@ -34,16 +34,17 @@ UNIT = "GRay·samples/s"
 CFG = dict(nx=256, ny=256, nz=256, voxel=1.0, nu=384, nv=384, pitch=1.2, n_views=64,
            sod=500.0, sdd=1000.0, iters=100, i0=1e5, seed=2024)
 
-# Bilinear fetches per second of one B200's texture units for a 32-bit texel
-# (dtv-net_b200/probes/texture_fetch_rate.cu: 3.84 fetches per clock per SM at
-# 1965 MHz). The projectors issue one such fetch per forward-projector sample
-# and per backprojected voxel-view.
-TEXTURE_FETCH_PEAK = 1.116e12
-
 # DRAM traffic of one forward-projector launch on this workload
-# (dram__bytes_read.sum + dram__bytes_write.sum, one ncu --set full capture of
-# `python bench.py --profile 12`) and that capture's texture-pipe utilisation.
-FP_NCU = {"pairs": {"traffic": 142.958336e6 + 26.171136e6, "tex_pipe_pct": 95.3}}
+# (dram__bytes_read.sum + dram__bytes_write.sum) and the texture-pipe
+# utilisation of that launch, from the ncu capture summarised in
+# profiles/fp_pair_kernel_sparse_view_dtv.md (`python bench.py --profile 12`).
+# They describe the kernel as captured there, not this run.
+FP_NCU = {"pairs": {"traffic": 142.958336e6 + 26.171136e6, "tex_pipe_pct": 95.3,
+                    "source": "profiles/fp_pair_kernel_sparse_view_dtv.md"}}
+
+# Same-FOV downsample on which the 100-iteration reconstruction is checked
+# against the FP64 oracle: 64^3 at 4 mm, 96x96 detector at 4.8 mm, 64 views.
+CHECK_DOWNSAMPLE = 4
 
 
 def workload_name(c):
@@ -266,6 +267,140 @@ def cpu_baseline(c, truth_np, views_per_step=2, steps=1, warmup=0):
     return total_units / elapsed / 1e9, cores, sample, elapsed
 
 
+def fp64_check(c, dev, sampler, prm, plan, truth, sino_clean, f_dtypes):
+    """Checker leg, outside every timed region: relative RMSE against the FP64
+    oracle of (1) the workload's forward projection of the phantom and (2) its
+    FDK backprojection, both at full size on 16 of the views, and (3) the
+    100-iteration reconstruction, on a same-FOV downsample by CHECK_DOWNSAMPLE
+    (edge, detector and views per FOV scaled together; 64 views kept), with the
+    same sampler, storage, step-size rule and noise model as the timed run."""
+    import numpy as np
+    import torch
+
+    import dtvb200
+    from dtvb200.phantom import ellipsoids, poisson_noise
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as O
+
+    def rel(a, b):
+        a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+        return float(np.sqrt(np.mean((a - b) ** 2) / np.mean(b ** 2)))
+
+    t0 = time.perf_counter()
+    ang = np.linspace(0, 360, c["n_views"], endpoint=False)
+    sel = list(range(0, c["n_views"], c["n_views"] // 16))
+    vs = (c["nx"], c["ny"], c["nz"])
+    geo_args = ((c["voxel"],) * 3, (c["nu"], c["nv"]), (c["pitch"], c["pitch"]), c["sod"], c["sdd"])
+    full = O.circular_geometry(ang, vs, *geo_args)
+    g_sel = O.circular_geometry(ang[sel], vs, *geo_args)
+    g_sel.og.bp_scale = full.og.bp_scale  # the full scan's FDK weight pi / N
+    vol = truth[0, 0].double().cpu().numpy()
+    fp_gpu = sino_clean[0, 0, sel].double().cpu().numpy()
+    e_fp = rel(fp_gpu, O.forward(g_sel, vol).reshape(fp_gpu.shape))
+    s_in = torch.zeros_like(sino_clean)
+    s_in[:, :, sel] = sino_clean[:, :, sel]
+    bp_gpu = plan.backward(s_in).double().cpu().numpy().reshape(vol.shape)
+    e_bp = rel(bp_gpu, O.backward(g_sel, sino_clean[0, 0, sel].cpu().numpy()).reshape(vol.shape))
+
+    k = CHECK_DOWNSAMPLE
+    d = dict(c, nx=c["nx"] // k, ny=c["ny"] // k, nz=c["nz"] // k, voxel=c["voxel"] * k,
+             nu=c["nu"] // k, nv=c["nv"] // k, pitch=c["pitch"] * k)
+    dvs = (d["nx"], d["ny"], d["nz"])
+    dargs = ((d["voxel"],) * 3, (d["nu"], d["nv"]), (d["pitch"], d["pitch"]), d["sod"], d["sdd"])
+    geo_d = dtvb200.circular(ang, dvs, *dargs)
+    og_d = O.circular_geometry(ang, dvs, *dargs)
+    plan_d = dtvb200.Plan(geo_d, max_batch=1, sampler=sampler, device=dev)
+    truth_d = ellipsoids((d["nz"], d["ny"], d["nx"]), seed=c["seed"], device=dev)
+    sino_d = poisson_noise(plan_d.forward(truth_d), c["i0"], seed=c["seed"])
+    prm_d = dtv_params(plan_d, dev)
+    sino_np = sino_d.cpu().numpy()
+    fpo = lambda x: O.forward(og_d, x).reshape(x.shape[0], 1, *og_d.sino_shape)  # noqa: E731
+    bpo = lambda s: O.backward(og_d, s).reshape(s.shape[0], 1, *og_d.vol_shape)  # noqa: E731
+    ref = O.dtvcp_run(fpo, bpo, np.zeros((1, 1) + og_d.vol_shape), sino_np, dvs, c["iters"],
+                      prm_d["sigma"], prm_d["tau"], prm_d["mu"], prm_d["v"], quirk=prm_d["quirk"])
+    recon = {}
+    for name, fdt in f_dtypes:
+        pl = plan_d if fdt == torch.float32 or sampler != "pairs" else \
+            dtvb200.Plan(geo_d, max_batch=1, sampler=sampler, stage_f16=True, device=dev)
+        alg = dtvb200.DTVCP(pl, c["iters"], t_refresh=10, use_graph=True, f_dtype=fdt, **prm_d)
+        recon[name] = rel(alg.run(torch.zeros(pl.vol_shape(1), device=dev), sino_d).cpu().numpy(),
+                          ref)
+    return {
+        "forward_full_size": e_fp, "backward_full_size": e_bp,
+        "reconstruction": recon, "gate": 1e-3,
+        "how": (f"relative RMSE vs the FP64 oracle (OpenMP C, exact trilinear/bilinear). "
+                f"Projections: the {c['nx']}^3 phantom, {len(sel)} of {c['n_views']} views at "
+                f"full size. Reconstruction: {c['iters']} DTV-PDHG iterations on a same-FOV "
+                f"downsample ({d['nx']}^3 x {d['voxel']:g} mm, {d['nu']}x{d['nv']} det @ "
+                f"{d['pitch']:g} mm, {c['n_views']} views, Poisson I0={c['i0']:g}), same "
+                f"sampler, storage and step-size rule as the timed run; the oracle runs the "
+                f"reference loop (DTVCP.py:29-60) on the same noisy sinogram"),
+        "seconds": time.perf_counter() - t0,
+    }
+
+
+def reference_cuda_baseline(c, dev, truth, steps=3):
+    """Baseline leg: the reference's own CUDA projectors (its unmodified
+    forwardKernel.cu / backwardKernel.cu, compiled with the texture-object
+    shim into oracle/_ref) called through their pybind API exactly as
+    StandardGeometry.py calls them: one launch per view with a host .item()
+    read before each, a cudaArray copy of the input per call. Timed per call
+    beside this library's Standard-geometry plans on the same arrays, in the
+    reference's geometry convention (voxel = detector pixel x SID/SDD)."""
+    import importlib.machinery
+    import importlib.util
+
+    import numpy as np
+    import torch
+
+    import dtvb200
+    path = os.path.join(REPO, "oracle", "_ref", "JITStandardGeometry.so")
+    if not os.path.exists(path):
+        return {"unavailable": "oracle/_ref/JITStandardGeometry.so not built"}
+    loader = importlib.machinery.ExtensionFileLoader("JITStandardGeometry", path)
+    spec = importlib.util.spec_from_file_location("JITStandardGeometry", path, loader=loader)
+    ref = importlib.util.module_from_spec(spec)
+    loader.exec_module(ref)
+    vs, ds = (c["nx"], c["ny"], c["nz"]), (c["nu"], c["nv"])
+    angles = np.linspace(0, 360, c["n_views"], endpoint=False)  # StandardGeometry.py:6
+    at = torch.from_numpy(angles).to(dev)
+    vst, dst = torch.tensor(vs).to(dev), torch.tensor(ds).to(dev)
+    sid, sdd = c["sod"], c["sdd"]
+    stream = torch.cuda.current_stream(dev)
+    geo = dtvb200.standard(angles.astype(np.float32), vs, ds, sid, sdd)
+    samples = dtvb200.Plan(geo, max_batch=1, sampler="soft", device=dev).fp_samples()
+    bp_units = float(np.prod(vs)) * c["n_views"]
+    sino = torch.empty((1, 1, c["n_views"], ds[1], ds[0]), device=dev)
+
+    def timed(fwd, bwd):
+        fwd()
+        bwd()
+        tf = time_steps(fwd, steps, stream) / steps
+        tb = time_steps(bwd, steps, stream) / steps
+        return {"forward_ms": tf * 1e3, "backward_ms": tb * 1e3,
+                "value": (samples + bp_units) / (tf + tb) / 1e9}
+
+    out = {"unit": UNIT, "geometry": (f"reference convention: {vs[0]}^3 voxels of SID/SDD "
+                                      f"detector pixels, {c['n_views']} views of "
+                                      f"{ds[0]}x{ds[1]}, SID {sid:g}, SDD {sdd:g}"),
+           "note": ("samples counted as this library's plan counts them for that geometry "
+                    "(the reference marches about twice as many, from its alpha-range rule)")}
+    sino_ref = ref.forward(truth, at, vst, dst, sid, sdd, dev.index)
+    out["reference"] = timed(lambda: ref.forward(truth, at, vst, dst, sid, sdd, dev.index),
+                             lambda: ref.backward(sino_ref, at, vst, dst, sid, sdd, dev.index))
+    for smp in ("tex", "pairs"):
+        pl = dtvb200.Plan(geo, max_batch=1, sampler=smp, device=dev)
+        vol_out = torch.empty_like(truth)
+        out[f"ours_{smp}"] = timed(lambda: pl.forward(truth, out=sino),
+                                   lambda: pl.backward(sino_ref, out=vol_out))
+        diff = float(((pl.forward(truth) - sino_ref).double() ** 2).mean().sqrt()
+                     / (sino_ref.double() ** 2).mean().sqrt())
+        out[f"ours_{smp}"]["forward_rel_rmse_vs_reference"] = diff
+        del pl
+    out["speedup_pairs_vs_reference"] = out["ours_pairs"]["value"] / out["reference"]["value"]
+    return out
+
+
 def run_reference(args):
     ws, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
     if rank != 0:
@@ -308,6 +443,7 @@ def run_ours(args):
     if args.small:
         c.update(nx=64, ny=64, nz=64, nu=96, nv=96, n_views=16, iters=10)
     geo, truth, _ = make_problem(dev, c, c["seed"] + rank)
+    tex_peak = dtvb200._lib.measure_texture_fetch_rate(32)
     plan = dtvb200.Plan(geo, max_batch=1, sampler=args.sampler, device=dev)
     sino_clean = plan.forward(truth)
     sino = poisson_noise(sino_clean, c["i0"], seed=c["seed"] + rank)
@@ -389,7 +525,11 @@ def run_ours(args):
             del plain, pplan
         extra["speedup_vs_plain_fp32"] = recon_s / extra["plain_fp32_eager"]["recon_per_s"]
 
-    cpu = None
+    cpu = check = ref_cuda = None
+    if rank == 0 and ws == 1 and not args.no_check:
+        check = fp64_check(c, dev, args.sampler, prm, plan, truth, sino_clean,
+                           [("fp32_f", torch.float32), ("fp16_fbar", torch.float16)])
+        ref_cuda = reference_cuda_baseline(c, dev, truth)
     if rank == 0 and ws == 1 and not args.no_cpu:
         # 48 of the 64 views: about 10-20 s of FP64 work on the host cores
         v, cores, sample, _ = cpu_baseline(c, truth[0, 0].double().cpu().numpy(),
@@ -399,7 +539,9 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp16-staged/fp32-acc" if args.sampler in ("pairs", "tma") else "f32",
+        "data": "synthetic",
         "config": {"workload": workload_name(c), "parallelism": f"replicas x{ws}",
                    "sampler": args.sampler, "graph": "one CUDA graph per reconstruction",
                    "l2": "working set > L2 (volume, 4 dual volumes, sinograms ~0.5 GB)",
@@ -413,17 +555,22 @@ def run_ours(args):
                      "frac": achieved / hbm_peak,
                      "traffic": FP_NCU.get(args.sampler, {}).get("traffic"),
                      "texture_pipe_pct_of_peak": FP_NCU.get(args.sampler, {}).get("tex_pipe_pct"),
+                     "traffic_source": FP_NCU.get(args.sampler, {}).get("source"),
                      "kernel": "forward projector (staging + ray kernel)",
                      "algorithmic_bytes_per_launch": fp_bytes,
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                      "texture": {
                          "unit": "bilinear fetches/s",
-                         "peak": TEXTURE_FETCH_PEAK,
+                         "peak": tex_peak,
+                         "peak_source": ("measured in this run (dtv_measure_texture_fetch_rate, "
+                                         "32-bit texels)"),
                          "forward_achieved": fp_samples / (t_fp * 1e-3),
-                         "forward_frac": fp_samples / (t_fp * 1e-3) / TEXTURE_FETCH_PEAK,
+                         "forward_frac": fp_samples / (t_fp * 1e-3) / tex_peak,
                          "backward_achieved": V * n_views / (t_bp * 1e-3),
-                         "backward_frac": V * n_views / (t_bp * 1e-3) / TEXTURE_FETCH_PEAK}},
+                         "backward_frac": V * n_views / (t_bp * 1e-3) / tex_peak}},
+        "error_vs_fp64": check,
         "cpu_baseline": cpu,
+        "reference_cuda_baseline": ref_cuda,
         "clocks": clk.summary(),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": P * 4,
                 "d2h_bytes_per_step": V * 4},
@@ -779,6 +926,8 @@ def main():
     ap.add_argument("--small", action="store_true", help="64^3 smoke-size workload")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-check", action="store_true",
+                    help="skip the FP64 error check and the reference-CUDA baseline")
     ap.add_argument("--workload", choices=["sparse_dtv", "batch16", "train", "fista64",
                                            "large512"],
                     default="sparse_dtv",

@@ -17,7 +17,7 @@ _sys.path.insert(0, _os.path.dirname(_os.path.abspath(__file__)))
 import torch as _torch  # noqa: E402
 
 from dtvb200 import geometry as _geo  # noqa: E402
-from JITStandardGeometry import _host_list, _SAMPLER  # noqa: E402
+from JITStandardGeometry import _check_len, _host_values, _SAMPLER  # noqa: E402
 
 _plans = {}
 
@@ -26,13 +26,16 @@ def _plan(volumeSize, detectorSize, projectVector, device, batch):
     if not isinstance(projectVector, _torch.Tensor) or projectVector.dim() != 2 or \
             projectVector.shape[1] != 12:
         raise RuntimeError("project vector's shape must be [angle's number, 12]")
-    pv = projectVector.detach().to("cpu", _torch.float32).contiguous()
-    vs = _host_list(volumeSize, 3, "volume size")
-    ds = _host_list(detectorSize, 2, "detector size")
-    key = (pv.numpy().tobytes(), tuple(vs), tuple(ds), int(device))
+    _check_len(volumeSize, 3, "volume size")
+    _check_len(detectorSize, 2, "detector size")
+    ph, vh, dh = _host_values([projectVector, volumeSize, detectorSize])
+    pv = ph.astype("float32").reshape(-1, 12)
+    vs = [int(v) for v in vh]
+    ds = [int(v) for v in dh]
+    key = (pv.tobytes(), tuple(vs), tuple(ds), int(device))
     p = _plans.get(key)
     if p is None or p.max_batch < batch:
-        g = _geo.vector(pv.numpy(), vs, ds)
+        g = _geo.vector(pv, vs, ds)
         p = _geo.Plan(g, max_batch=max(batch, 1), sampler=_SAMPLER,
                       device=_torch.device("cuda", int(device)))
         _plans[key] = p

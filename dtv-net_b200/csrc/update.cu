@@ -19,6 +19,7 @@
 // 24-bit significands. After the last level the bin is a single value and
 // lambda follows in closed form from the counts and sums above it.
 #include <atomic>
+#include <cstddef>
 #include <math.h>
 
 #include <algorithm>
@@ -501,7 +502,10 @@ __global__ void __launch_bounds__(1024) l1_select_kernel(L1Chan* chans, int leve
     }
   }
   __syncthreads();
-  const int J = best;
+  // Below level 1 the parent bin passed the test at its lower edge, so the
+  // lowest bin of this level passes too in exact arithmetic; if the sums,
+  // added in another order, round just under the radius, take that bin.
+  const int J = (best < 0 && level > 1) ? 0 : best;
   if (!ch.done && J >= 0 && J >= t * per && J < t * per + per) {
     // this thread owns bin J: fix the new "above" totals
     double ca = c_above, ta = t_above;
@@ -526,30 +530,39 @@ __global__ void __launch_bounds__(1024) l1_select_kernel(L1Chan* chans, int leve
       ch.done = 1;
     }
   }
-  __syncthreads();
-  for (int q = 0; q < per; ++q) {  // leave the histogram zeroed for the next search
-    cnt[t * per + q] = 0;
-    sum[t * per + q] = 0;
-  }
 }
 
-// Resets channels for a new search: radius from device doubles, or
-// s_c * t[c] (a scale times a device constraint level).
-__global__ void l1_reset_kernel(L1Chan* chans, int C, const double* radius, const double* t,
-                                float s0, float s1, float s2) {
-  const int c = threadIdx.x;
+// Resets channels for a new search, one block per channel: radius from
+// device doubles, or s_c * t[c] (a scale times a device constraint level),
+// and every histogram bin of the three levels cleared, so a search starts
+// from a defined state whatever the workspace held before (fresh
+// cudaMalloc'd memory, or a search that stopped part-way).
+constexpr int kL1ResetThreads = 256;
+__global__ void __launch_bounds__(kL1ResetThreads)
+l1_reset_kernel(L1Chan* chans, int C, const double* radius, const double* t, float s0, float s1,
+                float s2) {
+  const int c = blockIdx.x;
   if (c >= C) return;
   L1Chan& ch = chans[c];
-  const float sc = c == 0 ? s0 : (c == 1 ? s1 : s2);
-  ch.radius = radius ? radius[c] : (double)sc * t[c];
-  ch.c_above = 0.0;
-  ch.t_above = 0.0;
-  ch.lambda = 0.0;
-  ch.prefix = 0;
-  ch.maxkey = 0;
-  ch.done = 0;
-  ch.thresh = 0.f;
+  // cnt1..cnt3 and sum1..sum3 are contiguous: 4096 32-bit and 4096 64-bit words
+  unsigned int* bins = ch.cnt1;
+  constexpr int kWords = (kL1B1 + kL1B2 + kL1B3) * (1 + 2);
+  for (int i = threadIdx.x; i < kWords; i += kL1ResetThreads) bins[i] = 0u;
+  if (threadIdx.x == 0) {
+    const float sc = c == 0 ? s0 : (c == 1 ? s1 : s2);
+    ch.radius = radius ? radius[c] : (double)sc * t[c];
+    ch.c_above = 0.0;
+    ch.t_above = 0.0;
+    ch.lambda = 0.0;
+    ch.prefix = 0;
+    ch.maxkey = 0;
+    ch.done = 0;
+    ch.thresh = 0.f;
+  }
 }
+static_assert(offsetof(L1Chan, sum3) + sizeof(((L1Chan*)0)->sum3) ==
+                  offsetof(L1Chan, cnt1) + (kL1B1 + kL1B2 + kL1B3) * 3 * sizeof(unsigned int),
+              "histogram words are contiguous");
 
 __global__ void l1_apply_kernel(const float* __restrict__ v, float* __restrict__ w, int64_t n,
                                 const L1Chan* ch, double* lambda_out) {
@@ -821,6 +834,23 @@ __global__ void axpy_l1_kernel(float* __restrict__ f, const float* __restrict__ 
   if (l1) block_sums_atomic<1>(acc, l1);
 }
 
+// sum += sum |a - b| (FP64 accumulation): ASD-POCS's TV-change measure.
+__global__ void l1_distance_kernel(const float* __restrict__ a, const float* __restrict__ b,
+                                   double* sum, int64_t n) {
+  double acc[1] = {0.0};
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x)
+    acc[0] += fabsf(__ldg(a + t) - __ldg(b + t));
+  block_sums_atomic<1>(acc, sum);
+}
+
+// ASD-POCS step-size rule on the device: davg *= alpha when the TV steps
+// moved the iterate more than rmax times the data step did.
+__global__ void asd_adapt_kernel(const double* dp_sum, const double* dg_sum, float rmax,
+                                 float alpha, float* davg) {
+  if (threadIdx.x == 0 && *dg_sum > (double)rmax * *dp_sum) *davg *= alpha;
+}
+
 __device__ __forceinline__ void grad3(const float* f, const Dims& d, int64_t i, int x, int y, int z,
                                       float g[3]) {
 #pragma unroll
@@ -908,7 +938,7 @@ int dtv_l1ball(const float* v, float* w, int64_t n, const double* radius, void* 
   DTV_CHECK(n <= 2147483647LL, "n = %lld exceeds 2^31-1 (32-bit bin counts)", (long long)n);
   cudaStream_t st = as_stream(stream);
   L1Chan* ch = reinterpret_cast<L1Chan*>(ws);
-  l1_reset_kernel<<<1, 32, 0, st>>>(ch, 1, radius, nullptr, 0.f, 0.f, 0.f); note_launch();
+  l1_reset_kernel<<<1, kL1ResetThreads, 0, st>>>(ch, 1, radius, nullptr, 0.f, 0.f, 0.f); note_launch();
   l1_hist1_kernel<<<hist_blocks(n, 256, 4, 1), 256, 0, st>>>(v, n, ch); note_launch();
   l1_select_kernel<<<1, 1024, 0, st>>>(ch, 1); note_launch();
   l1_hist_kernel<1><<<hist_blocks(n, 256, 4, 1), 256, 0, st>>>(v, nullptr, nullptr, n, ch, 2); note_launch();
@@ -947,7 +977,7 @@ int dtv_pdhg_dual(const void* fbar, float* p, float* q, float* s, float* c, cons
   const int64_t per_block = kHistBlockElems / (kTX * kTY * kDualZS);
   const int grid = (int)std::max<int64_t>(std::min<int64_t>(tiles, 148LL * 6),
                                           (tiles + per_block - 1) / per_block);
-  l1_reset_kernel<<<1, 32, 0, st>>>(ch, 3, nullptr, t, sg * prm->v[0], sg * prm->v[1],
+  l1_reset_kernel<<<3, kL1ResetThreads, 0, st>>>(ch, 3, nullptr, t, sg * prm->v[0], sg * prm->v[1],
                                     sg * prm->v[2]); note_launch();
   if (prm->f_dtype == DTV_F32) {
     pdhg_dual_kernel<float><<<grid, kBlock3, 0, st>>>(
@@ -1100,6 +1130,21 @@ int dtv_tv_descent(const float* f_in, float* f_out, const int32_t size[3], int32
   return DTV_OK;
 }
 
+int dtv_l1_distance(const float* a, const float* b, int64_t n, double* sum, void* stream) {
+  DTV_CHECK(a && b && sum && n > 0, "bad argument");
+  l1_distance_kernel<<<blocks_for(n), 256, 0, as_stream(stream)>>>(a, b, sum, n); note_launch();
+  DTV_LAUNCH_CHECK();
+  return DTV_OK;
+}
+
+int dtv_asd_adapt(const double* dp_sum, const double* dg_sum, float rmax, float alpha,
+                  float* davg, void* stream) {
+  DTV_CHECK(dp_sum && dg_sum && davg, "NULL argument");
+  asd_adapt_kernel<<<1, 32, 0, as_stream(stream)>>>(dp_sum, dg_sum, rmax, alpha, davg); note_launch();
+  DTV_LAUNCH_CHECK();
+  return DTV_OK;
+}
+
 int dtv_scale_scalar(const double* in, double scale, float* out, void* stream) {
   DTV_CHECK(in && out, "NULL argument");
   scale_scalar_kernel<<<1, 32, 0, as_stream(stream)>>>(in, scale, out); note_launch();
@@ -1166,7 +1211,7 @@ extern "C" int dtv_l1ball_noalloc(const float* v, float* w, int64_t n, const dou
   // The array keeps whatever the previous call left; the histograms must
   // start at zero, so clear the whole workspace first.
   DTV_CUDA_TRY(cudaMemsetAsync(ch, 0, sizeof(L1Chan), st));
-  l1_reset_kernel<<<1, 32, 0, st>>>(ch, 1, radius, nullptr, 0.f, 0.f, 0.f); note_launch();
+  l1_reset_kernel<<<1, kL1ResetThreads, 0, st>>>(ch, 1, radius, nullptr, 0.f, 0.f, 0.f); note_launch();
   l1_hist1_kernel<<<hist_blocks(n, 256, 4, 1), 256, 0, st>>>(v, n, ch); note_launch();
   l1_select_kernel<<<1, 1024, 0, st>>>(ch, 1); note_launch();
   l1_hist_kernel<1><<<hist_blocks(n, 256, 4, 1), 256, 0, st>>>(v, nullptr, nullptr, n, ch, 2); note_launch();

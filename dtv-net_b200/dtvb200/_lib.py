@@ -106,6 +106,10 @@ SIGNATURES = {
     "dtv_axpy_l1": [_P, _P, _F, _P, _L, _P],
     "dtv_tv_descent": [_P, _P, _IP, _I, _I, _P, _P],
     "dtv_scale_scalar": [_P, _D, _P, _P],
+    "dtv_l1_distance": [_P, _P, _L, _P, _P],
+    "dtv_asd_adapt": [_P, _P, _F, _F, _P, _P],
+    "dtv_measure_texture_fetch_rate": [_I, _DP],
+    "dtv_measure_atomic_v4_rate": [_L, _I, _DP],
 }
 _RESTYPES = {
     "dtv_error_string": ctypes.c_char_p,
@@ -143,6 +147,20 @@ def call(name: str, *args) -> int:
         msg = L.dtv_last_error_message().decode(errors="replace")
         raise DtvError(name, rc, msg)
     return rc
+
+
+def measure_texture_fetch_rate(texel_bits: int = 32) -> float:
+    """Bilinear texture fetches per second of the current device (benchmarks)."""
+    out = ctypes.c_double()
+    call("dtv_measure_texture_fetch_rate", texel_bits, ctypes.byref(out))
+    return out.value
+
+
+def measure_atomic_v4_rate(records: int = 72 << 16, pattern: int = 0) -> float:
+    """16-byte vector reductions per second into L2-resident records (benchmarks)."""
+    out = ctypes.c_double()
+    call("dtv_measure_atomic_v4_rate", records, pattern, ctypes.byref(out))
+    return out.value
 
 
 def ivec(vals) -> ctypes.Array:

@@ -459,13 +459,16 @@ class ASDPOCS(_Graphable):
     """ASD-POCS (model/PDHG/ASDPOCS.py:28-47): a Landweber data step, then
     ``ng`` normalised-TV steepest-descent steps of length davg, davg = alpha*dp
     from the first data step. With quirk=True (the reference's behaviour) f0
-    aliases f, the TV-change test never fires and davg stays fixed."""
+    aliases f, the TV-change test never fires and davg stays fixed. With
+    quirk=False f0 is a copy of the data-step result, dp = mean|f_prev - f|
+    of every data step and dg = mean|f - f0| after the TV steps, and davg is
+    multiplied by alpha whenever dg > rmax * dp (:44-45), all on the device;
+    the TV steps then also use the clean D_y (no wrap into the next z-slice,
+    Gradients.py:18-25), as in DTVCP's quirk=False."""
 
     def __init__(self, plan: Plan, cascades: int = 30, beta: float = 0.00005,
                  beta_red: float = 0.9999, ng: int = 10, alpha: float = 0.001, rmax: float = 0.95,
                  alpha_red: float = 0.95, quirk: bool = True, use_graph: bool = False):
-        if not quirk:
-            raise NotImplementedError("only the reference's (aliased f0) behaviour is built")
         self.plan = plan
         self.cascades = int(cascades)
         self.beta, self.beta_red = float(beta), float(beta_red)
@@ -483,18 +486,28 @@ class ASDPOCS(_Graphable):
         f, f2 = st["f"], st["f2"]
         f.copy_(st["img"])
         beta = self.beta
+        dy_quirk = 1 if self.quirk else 0
         for i in range(self.cascades):
             plan.forward(f, out=st["r"], epilogue=_lib.DTV_EPI_RESIDUAL, g=st["g"])
             plan.backward(st["r"], out=st["bp"])
-            if i == 0:
+            track = i == 0 or not self.quirk
+            if track:
                 st["l1"].zero_()
-            call("dtv_axpy_l1", _ptr(f), _ptr(st["bp"]), beta, _ptr(st["l1"]) if i == 0 else None,
+            call("dtv_axpy_l1", _ptr(f), _ptr(st["bp"]), beta, _ptr(st["l1"]) if track else None,
                  n, stream)
             if i == 0:  # davg = alpha * mean|f0 - f|   (:34-35)
                 call("dtv_scale_scalar", _ptr(st["l1"]), self.alpha / n, _ptr(st["davg"]), stream)
+            if not self.quirk:
+                st["f0"].copy_(f)  # f0 = f, a copy (:36)
             for _ in range(self.ng):
-                call("dtv_tv_descent", _ptr(f), _ptr(f2), size, b, 1, _ptr(st["davg"]), stream)
+                call("dtv_tv_descent", _ptr(f), _ptr(f2), size, b, dy_quirk, _ptr(st["davg"]),
+                     stream)
                 f, f2 = f2, f
+            if not self.quirk:  # dg = mean|f - f0|; davg *= alpha if dg > rmax * dp (:44-45)
+                st["dg"].zero_()
+                call("dtv_l1_distance", _ptr(f), _ptr(st["f0"]), n, _ptr(st["dg"]), stream)
+                call("dtv_asd_adapt", _ptr(st["l1"]), _ptr(st["dg"]), self.rmax, self.alpha,
+                     _ptr(st["davg"]), stream)
             beta *= self.beta_red
         st["result"] = f
 
@@ -504,8 +517,9 @@ class ASDPOCS(_Graphable):
         st = self.__dict__.setdefault("_state", {}).get(key)
         if st is None:
             b = image.shape[0]
-            st = {k: torch.empty_like(image) for k in ("f", "f2", "bp", "img")}
+            st = {k: torch.empty_like(image) for k in ("f", "f2", "bp", "img", "f0")}
             st["b"] = b
+            st["dg"] = torch.zeros(1, dtype=torch.float64, device=image.device)
             st["r"] = torch.empty(self.plan.sino_shape(b), dtype=torch.float32,
                                   device=image.device)
             st["g"] = torch.empty_like(st["r"])

@@ -66,39 +66,79 @@ class Projector:
         return self.plan(x.device, self.batch_of(x, True), sampler="soft").forward(x)
 
 
-def make_functions(projector: Projector, matched: bool = False):
+def plane_layout(geometry: Geometry, planes: int = None):
+    """(to_layer, from_layer): the Beijing layers' sinogram layout.
+
+    The projector's sinogram is [B,1,A*P,H,W] in (angle, plane, row, column)
+    order. With ``planes`` = P, the Beijing layers hand out the same shape
+    holding (angle, row, plane, column): each angle's H rows run across all P
+    sub-detectors, as BeijingGeometry.py:18,23,31,39 permute it. Without
+    ``planes`` both maps are the identity."""
+    if not planes:
+        return (lambda s: s), (lambda s: s)
+    W, H = geometry.detector_size
+    N = geometry.n_views
+    if N % planes:
+        raise ValueError(f"{N} views are not a whole number of angles of {planes} planes")
+    A, P = N // planes, int(planes)
+
+    def to_layer(s):
+        B = s.shape[0]
+        return s.reshape(B, A, P, H, W).permute(0, 1, 3, 2, 4).reshape(B, 1, N, H, W)
+
+    def from_layer(s):
+        B = s.shape[0]
+        return s.reshape(B, A, H, P, W).permute(0, 1, 3, 2, 4).reshape(B, 1, N, H, W)
+
+    return to_layer, from_layer
+
+
+def make_functions(projector: Projector, matched: bool = False, planes: int = None,
+                   sample_interval: float = 1.0):
     """(ForwardProjection, BackProjection) autograd Functions bound to a
-    projector, with the reference pairing or the matched-adjoint pairing."""
+    projector, with the reference pairing or the matched-adjoint pairing.
+
+    ``planes`` and ``sample_interval`` give the Beijing layers' conventions
+    (BeijingGeometry.py:13-39): sinograms in the layout of ``plane_layout``,
+    and the forward projection scaled by the sample interval. As in the
+    reference pairing, that scale multiplies ForwardProjection.forward and
+    BackProjection.backward only (the FDK backprojector is unscaled); in the
+    matched pairing the transposes carry it, so each pair stays exact."""
+    to_layer, from_layer = plane_layout(projector.geometry, planes)
+    s = float(sample_interval)
+
+    def scaled(t):
+        return t if s == 1.0 else t * s
+
+    def fwd(x):
+        return to_layer(scaled(projector.fp_soft(x) if matched else projector.fp(x)))
+
+    def back(y):
+        y = from_layer(y)
+        return scaled(projector.adjoint(y)) if matched else projector.bp(y)
 
     class ForwardProjection(torch.autograd.Function):
-        """StandardGeometry.py:10-21."""
+        """StandardGeometry.py:10-21, BeijingGeometry.py:13-26."""
 
         @staticmethod
         def forward(ctx, input):
-            if matched:
-                return projector.fp_soft(input)
-            return projector.fp(input)
+            return fwd(input)
 
         @staticmethod
         def backward(ctx, grad):
-            if matched:
-                return projector.adjoint(grad)
-            return projector.bp(grad)
+            return back(grad)
 
     class BackProjection(torch.autograd.Function):
-        """StandardGeometry.py:23-34 (matched: the adjoint A^T)."""
+        """StandardGeometry.py:23-34, BeijingGeometry.py:28-39 (matched: the
+        adjoint A^T)."""
 
         @staticmethod
         def forward(ctx, input):
-            if matched:
-                return projector.adjoint(input)
-            return projector.bp(input)
+            return back(input)
 
         @staticmethod
         def backward(ctx, grad):
-            if matched:
-                return projector.fp_soft(grad)
-            return projector.fp(grad)
+            return fwd(grad)
 
     return ForwardProjection, BackProjection
 
@@ -117,17 +157,21 @@ class StandardGeometry(torch.nn.Module):
 
 
 class BeijingGeometry(torch.nn.Module):
-    """-lamb * BP(FP(x) - p)  (BeijingGeometry.py:41-48)."""
+    """-lamb * BP(FP(x) - p)  (BeijingGeometry.py:41-48), with the Beijing
+    autograd pair: the forward projection times ``sample_interval`` and, with
+    ``planes``, sinograms in the (angle, row, plane, column) layout the
+    reference's layer uses (``plane_layout``)."""
 
     def __init__(self, projector: Projector, matched: bool = False, lamb: float = 10e-3,
-                 sample_interval: float = 1.0):
+                 sample_interval: float = 1.0, planes: int = None):
         super().__init__()
-        self.FP, self.BP = make_functions(projector, matched)
+        self.FP, self.BP = make_functions(projector, matched, planes, sample_interval)
         self.lamb = lamb
         self.sample_interval = sample_interval
+        self.planes = planes
 
     def forward(self, x, p):
-        residual = self.FP.apply(x) * self.sample_interval - p
+        residual = self.FP.apply(x) - p
         return -self.lamb * self.BP.apply(residual)
 
 
@@ -209,18 +253,21 @@ class StandardGeometryWithFBP(torch.nn.Module):
 
 
 class BeijingGeometryWithFBP(torch.nn.Module):
-    """x - lamb * BP(filtered residual)  (BeijingGeometry.py:50-72). As the
-    reference, the residual [1,1,A*planes,H,W] is reinterpreted as rows of
-    W*planes columns (A views of H rows), weighted with the reference's
-    midpoints (row offset from W*planes/2, column offset from H/2,
-    BeijingGeometry.py:66-72) and ramp-filtered along those rows."""
+    """x - lamb * BP(filtered residual)  (BeijingGeometry.py:50-72). The
+    residual comes in the layer layout (angle, row, plane, column), so each
+    angle's rows span the W*planes columns of all sub-detectors; as in the
+    reference it is weighted with the reference's midpoints (row offset from
+    W*planes/2, column offset from H/2, BeijingGeometry.py:66-72) and
+    ramp-filtered along those rows, then backprojected through the layer's
+    BackProjection (which undoes the layout)."""
 
-    def __init__(self, projector: Projector, sdd: float, planes: int, matched: bool = False):
+    def __init__(self, projector: Projector, sdd: float, planes: int, matched: bool = False,
+                 sample_interval: float = 1.0):
         super().__init__()
         g = projector.geometry
         if g.n_views % planes:
             raise ValueError("the view count must be a multiple of planes")
-        self.FP, self.BP = make_functions(projector, matched)
+        self.FP, self.BP = make_functions(projector, matched, planes, sample_interval)
         self.lamb = torch.nn.Parameter(torch.tensor(1.0), requires_grad=False)
         self.width, self.height = g.detector_size
         self.planes, self.angles = int(planes), g.n_views // planes
@@ -237,7 +284,7 @@ class BeijingGeometryWithFBP(torch.nn.Module):
     def forward(self, x, p):
         residual = self.FP.apply(x) - p
         shape = residual.shape
-        rows = residual.reshape(1, 1, self.angles, self.height, self.width * self.planes)
+        rows = residual.reshape(shape[0], 1, self.angles, self.height, self.width * self.planes)
         rows = RampFilter.apply(rows, self.sdd, self.height, self.width * self.planes / 2,
                                 self.height / 2)
         return x - self.lamb * self.BP.apply(rows.reshape(shape))

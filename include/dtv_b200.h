@@ -304,7 +304,8 @@ DTV_API int64_t dtv_l1ball_workspace_bytes(void);
  * sum max(|v| - lambda, 0) = radius, or w = v when sum|v| < radius
  * (model/PDHG/Utils/L1ball.py:4-17, which Newton-iterates lambda with a host
  * sync per step; here an exact 3-pass radix search on the device).
- * radius: device double. workspace: dtv_l1ball_workspace_bytes() bytes.
+ * radius: device double. workspace: dtv_l1ball_workspace_bytes() bytes of
+ * device memory, 8-byte aligned, any contents (the call clears what it uses).
  * lambda_out (device double, may be NULL) receives lambda. */
 DTV_API int dtv_l1ball(const float* v, float* w, int64_t n, const double* radius, void* workspace,
                double* lambda_out, void* stream);
@@ -320,7 +321,10 @@ DTV_API int dtv_l1ball(const float* v, float* w, int64_t n, const double* radius
  * looks up that array's address; make the first call before any stream
  * capture. All calls on a device share the array, so calls that overlap on
  * the GPU (different streams, or different host threads) race; each call
- * clears it before use. Allocates nothing. */
+ * clears it before use. The address is cached per device ordinal for the
+ * life of the library: do not call it after cudaDeviceReset (or any other
+ * teardown of the device's primary context) in the same process. Allocates
+ * nothing. */
 DTV_API int dtv_l1ball_noalloc(const float* v, float* w, int64_t n, const double* radius,
                                double* lambda_out, void* stream);
 
@@ -335,7 +339,9 @@ typedef struct dtv_pdhg_params {
                       (f itself is always FP32) */
 } dtv_pdhg_params;
 
-/* Workspace bytes of the fused dual step (three L1-ball channels). */
+/* Workspace bytes of the fused dual step (three L1-ball channels). The
+ * workspace is device memory, 8-byte aligned, of any contents: the dual step
+ * clears it, and the primal step reads the thresholds the dual step left. */
 DTV_API int64_t dtv_pdhg_workspace_bytes(void);
 /* Dual step, fused: p_ = p + v1*sigma*D_x fbar (q_, s_ likewise, stored in
  * place), c = -relu(-c - sigma*mu*fbar), then the per-direction L1-ball
@@ -392,6 +398,31 @@ DTV_API int dtv_tv_descent(const float* f_in, float* f_out, const int32_t size[3
 /* out[0] = (float)(in[0] * scale) on the device (scalar glue that keeps
  * data-dependent step sizes such as davg = alpha * dp on the GPU, ASDPOCS.py:35). */
 DTV_API int dtv_scale_scalar(const double* in, double scale, float* out, void* stream);
+
+/* sum[0] += sum |a - b| over n elements (device double): ASD-POCS's
+ * l1_loss(f, f0) as a sum (model/PDHG/ASDPOCS.py:44). */
+DTV_API int dtv_l1_distance(const float* a, const float* b, int64_t n, double* sum, void* stream);
+/* davg[0] *= alpha if dg_sum[0] > rmax * dp_sum[0], on the device, so the
+ * adaptive step needs no host sync (ASDPOCS.py:45; dp and dg as sums over the
+ * same n elements). */
+DTV_API int dtv_asd_adapt(const double* dp_sum, const double* dg_sum, float rmax, float alpha,
+                          float* davg, void* stream);
+
+/* ---- roofline denominators (benchmarks only) ------------------------------------
+ * No counterpart in the reference, which times nothing. The projectors are
+ * bound by the texture unit and the exact adjoint by L2 vector reductions, not
+ * by HBM; these time each rate on the current device with a kernel that does
+ * nothing else. Both allocate, launch on the legacy default stream and
+ * synchronise: do not call them inside a stream capture or on a hot path. */
+/* Bilinear fetches per second from a layered 2-D texture of 384 x 384 x 64
+ * texels: texel_bits 32 (half2, the forward projector's z-pair texel, and the
+ * rate of the FP32 sinogram texels) or 64 (half4). */
+DTV_API int dtv_measure_texture_fetch_rate(int32_t texel_bits, double* fetches_per_second);
+/* 16-byte float4 atomicAdd reductions per second into `records` records
+ * ([1024, 2^26]; 72 MB = 4.7M records stays in L2): pattern 0, each warp's
+ * 32 lanes on 32 consecutive records (the adjoint's neighbouring rays);
+ * pattern 1, every lane on a random record. */
+DTV_API int dtv_measure_atomic_v4_rate(int64_t records, int32_t pattern, double* atomics_per_second);
 
 #ifdef __cplusplus
 }

@@ -80,16 +80,21 @@ def test_fbp_layer_gradient_is_the_transpose(cuda):
 
 
 def test_beijing_fbp_layer_matches_reference_formulation(cuda):
-    planes, angles, W, H = 3, 4, 10, 8
+    """BeijingGeometry.py:17-18,31,38-39,57-64 restated in torch ops on the same
+    projector: FP x sampleInterval, (view, plane) permutation, cosine weight
+    and ramp along rows of W*planes, permutation back, FDK BP."""
+    planes, angles, W, H, si = 3, 7, 10, 8, 1.7
     pv = vector_views(angles * planes, 40.0, 70.0, 1.6, 1.7)
     geo = dtvb200.vector(pv, (16, 14, 10), (W, H))
     proj = dtvb200.Projector(geo)
-    layer = dtvb200.BeijingGeometryWithFBP(proj, 70.0, planes).to(cuda)
+    layer = dtvb200.BeijingGeometryWithFBP(proj, 70.0, planes, sample_interval=si).to(cuda)
     rng = np.random.default_rng(5)
     x = torch.from_numpy(rng.random(geo.vol_shape(1)).astype(np.float32)).to(cuda)
     p = torch.from_numpy(rng.random(geo.sino_shape(1)).astype(np.float32)).to(cuda)
     out = layer(x, p)
-    res = (proj.fp(x) - p).view(1, 1, angles, H, W * planes) * layer.cosWeight
+    fp = (proj.fp(x) * si).reshape(angles, planes, H, W).permute(0, 2, 1, 3)
+    res = (fp.reshape(1, 1, angles * planes, H, W) - p).view(1, 1, angles, H, W * planes)
+    res = res * layer.cosWeight
     prev = torch.backends.cudnn.allow_tf32
     torch.backends.cudnn.allow_tf32 = False
     try:
@@ -97,5 +102,7 @@ def test_beijing_fbp_layer_matches_reference_formulation(cuda):
                                          padding=(0, W * planes // 2))
     finally:
         torch.backends.cudnn.allow_tf32 = prev
-    ref = x - layer.lamb * proj.bp(res.view(1, 1, angles * planes, H, W).contiguous())
+    back = res.reshape(angles, H, planes, W).permute(0, 2, 1, 3).reshape(1, 1, angles * planes,
+                                                                            H, W)
+    ref = x - layer.lamb * proj.bp(back.contiguous())
     assert rel_rmse(out.cpu().numpy(), ref.cpu().numpy()) < 1e-5

@@ -140,3 +140,21 @@ def test_large_scan_downsample_gate(cuda):
                   torch.from_numpy(ref.astype(np.float32)).to(cuda)).cpu().numpy()
     assert rel_rmse(rec, rec_ref) < GATE
 
+
+
+def test_headline_fp64_check(cuda):
+    """The FP64 check that bench.py prints beside the headline number, run as a
+    test: the sparse-view DTV workload's forward projection and FDK
+    backprojection of its phantom at full size (16 of 64 views), and its
+    100-iteration reconstruction on the same-FOV 64^3 downsample with FP32 and
+    FP16 fbar storage, each within 1e-3 relative RMSE of the FP64 oracle."""
+    import bench
+    c = dict(bench.CFG)
+    geo, truth, _ = bench.make_problem(cuda, c, c["seed"])
+    plan = dtvb200.Plan(geo, max_batch=1, sampler="pairs", device=cuda)
+    sino_clean = plan.forward(truth)
+    chk = bench.fp64_check(c, cuda, "pairs", None, plan, truth, sino_clean,
+                           [("fp32_f", torch.float32), ("fp16_fbar", torch.float16)])
+    assert chk["forward_full_size"] < GATE and chk["backward_full_size"] < GATE
+    for name, e in chk["reconstruction"].items():
+        assert e < GATE, (name, e)

@@ -438,10 +438,15 @@ def test_standard_layers_autograd(cuda):
     x.grad = None
     FPm.apply(x).backward(gy)
     assert torch.allclose(x.grad, proj.adjoint(gy), rtol=1e-4, atol=1e-5)
-    layer = dtvb200.StandardGeometry(proj, matched=True)
     p = torch.rand_like(y)
-    out = layer(x.detach(), p)
-    assert out.shape == x.shape
+    # the layer's value: x - lamb * BP(FP(x) - p)  (StandardGeometry.py:41-43)
+    xn, pn = x.detach().cpu().numpy(), p.cpu().numpy()
+    for matched, bp in ((False, O.backward), (True, O.adjoint)):
+        layer = dtvb200.StandardGeometry(proj, matched=matched, lamb=0.7)
+        out = layer(x.detach(), p)
+        res = O.forward(og, xn).reshape(pn.shape) - pn
+        ref = xn - 0.7 * bp(og, res).reshape(xn.shape)
+        assert rel_rmse(out.cpu().numpy(), ref) < 1e-5
 
 
 def test_gradcheck_matched_on_random_voxels(cuda):

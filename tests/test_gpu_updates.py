@@ -85,6 +85,73 @@ def test_l1ball_exact_on_large_inputs(cuda, n, scale, frac):
             assert s == 0.0
 
 
+def _l1ball_ws(v, radius, ws, cuda):
+    from dtvb200.geometry import _ptr, _stream
+    w = torch.empty_like(v)
+    lam = torch.empty(1, dtype=torch.float64, device=cuda)
+    _lib.call("dtv_l1ball", _ptr(v), _ptr(w), v.numel(), _ptr(radius), _ptr(ws), _ptr(lam),
+              _stream(cuda))
+    return w, lam
+
+
+@pytest.mark.parametrize("fill", [0xFF, 0x5A, 0x01])
+def test_l1ball_workspace_of_any_contents(cuda, fill):
+    """A caller's workspace need not be zeroed (a fresh cudaMalloc, or one a
+    previous search left part-way): the call clears what it uses."""
+    rng = np.random.default_rng(fill)
+    n = 300_001
+    v = dev_t((rng.standard_normal(n) * 3.0).astype(np.float32), cuda)
+    nbytes = _lib.load().dtv_l1ball_workspace_bytes()
+    for frac in (0.2, 0.7):
+        radius = torch.tensor([frac * float(v.double().abs().sum())], dtype=torch.float64,
+                              device=cuda)
+        w0, l0 = _l1ball_ws(v, radius, torch.zeros(nbytes, dtype=torch.uint8, device=cuda), cuda)
+        dirty = torch.full((nbytes,), fill, dtype=torch.uint8, device=cuda)
+        w1, l1 = _l1ball_ws(v, radius, dirty, cuda)
+        assert torch.equal(w0, w1) and torch.equal(l0, l1)
+        lam_ref = O.l1ball_lambda_exact(v.cpu().numpy(), float(radius))
+        assert abs(float(l1) - lam_ref) <= 1e-6 * lam_ref
+
+
+@pytest.mark.parametrize("edge", [0.5, 0.25, 2.0 ** -20])
+def test_l1ball_radius_on_a_bin_edge(cuda, edge):
+    """lambda falls exactly on a power of two, the lower edge of a bin at every
+    level of the radix search."""
+    k = 17
+    v = np.concatenate([np.full(k, 2 * edge), np.full(k, -edge), np.full(5, edge / 2),
+                        np.zeros(9)]).astype(np.float32)
+    np.random.default_rng(3).shuffle(v)
+    b = k * edge  # sum max(|v| - edge, 0) = k * edge
+    out, lam = dtvb200.l1ball(dev_t(v, cuda), b)
+    assert float(lam) == pytest.approx(edge, rel=1e-7)
+    ref = np.sign(v) * np.maximum(np.abs(v) - edge, 0)
+    assert np.abs(out.cpu().numpy() - ref).max() <= 1e-7 * edge
+
+
+def test_pdhg_dual_workspace_of_any_contents(cuda):
+    import ctypes
+    from dtvb200.geometry import _ptr, _stream
+    vs, fbar, f, (p, q, s, c), recon, prm, t = _pdhg_case(cuda)
+    tt = torch.tensor(t, dtype=torch.float64, device=cuda)
+    nbytes = _lib.load().dtv_pdhg_workspace_bytes()
+    outs = []
+    for fill in (0x00, 0xFF, 0x3C):
+        ws = torch.full((nbytes,), fill, dtype=torch.uint8, device=cuda)
+        T = {k: dev_t(x, cuda) for k, x in dict(fbar=fbar, f=f, p=p, q=q, s=s, c=c,
+                                                  recon=recon).items()}
+        size = _lib.ivec(vs)
+        _lib.call("dtv_pdhg_dual", _ptr(T["fbar"]), _ptr(T["p"]), _ptr(T["q"]), _ptr(T["s"]),
+                  _ptr(T["c"]), size, 1, ctypes.byref(prm), _ptr(tt), _ptr(ws), _stream(cuda))
+        _lib.call("dtv_pdhg_primal", _ptr(T["f"]), _ptr(T["fbar"]), _ptr(T["recon"]),
+                  _ptr(T["p"]), _ptr(T["q"]), _ptr(T["s"]), _ptr(T["c"]), size, 1,
+                  ctypes.byref(prm), _ptr(ws), _stream(cuda))
+        torch.cuda.synchronize()
+        outs.append([T[k].cpu() for k in ("p", "q", "s", "c", "f", "fbar")])
+    for o in outs[1:]:
+        for a, b in zip(outs[0], o):
+            assert torch.equal(a, b)
+
+
 def _pdhg_case(cuda, fdt=torch.float32, quirk=True):
     rng = np.random.default_rng(5)
     vs = (20, 16, 12)
@@ -217,6 +284,27 @@ def test_asdpocs_matches_reference(cuda):
                           rmax=p[4])
     f = alg.run(torch.zeros(plan.vol_shape(1), device=cuda), dev_t(z["loop_sino"], cuda))
     assert rel_rmse(f.cpu().numpy(), z["asd_f"]) < 1e-4
+
+
+@pytest.mark.parametrize("alpha", [0.001, 0.2])
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_asdpocs_clean_mode_matches_oracle(cuda, alpha, use_graph):
+    """quirk=False: f0 is a real copy, so the TV-change test of ASDPOCS.py:44-45
+    runs (with alpha = 0.2 it fires and shrinks davg; the result then differs
+    from the aliased reference run by about 2%), and D_y does not wrap."""
+    M, z, plan, fp, bp = _loop(cuda)
+    p = z["asd_params"]
+    alg = dtvb200.ASDPOCS(plan, int(p[5]), beta=p[0], beta_red=p[1], ng=int(p[2]), alpha=alpha,
+                          rmax=p[4], quirk=False, use_graph=use_graph)
+    f = alg.run(torch.zeros(plan.vol_shape(1), device=cuda), dev_t(z["loop_sino"], cuda))
+    img = np.zeros((1, 1) + plan.vol_shape(1)[2:])
+    fo = O.asdpocs_run(fp, bp, img, z["loop_sino"], M.LOOP_VS, int(p[5]), p[0], p[1], int(p[2]),
+                       alpha, p[4], quirk=False)
+    assert rel_rmse(f.cpu().numpy(), fo) < 1e-4
+    if alpha == 0.2:
+        fq = O.asdpocs_run(fp, bp, img, z["loop_sino"], M.LOOP_VS, int(p[5]), p[0], p[1],
+                           int(p[2]), alpha, p[4], quirk=True)
+        assert rel_rmse(f.cpu().numpy(), fq) > 1e-2
 
 
 def test_power_norm_close_to_two(cuda):

@@ -55,6 +55,30 @@ def test_noalloc_matches_workspace_entry_two_calls(cuda):
         assert float(w.double().abs().sum()) == pytest.approx(float(radius), rel=1e-5)
 
 
+def test_noalloc_against_fp64_after_an_early_exit(cuda):
+    """Checked against the FP64 threshold of the oracle rather than against the
+    kernels it shares with dtv_l1ball. The first call has sum|v| < radius (the
+    search stops at level 1 and returns v); the next call on the same shared
+    array is an ordinary projection."""
+    import oracle as O
+    rng = np.random.default_rng(7)
+    v1 = torch.from_numpy(rng.standard_normal(50_000).astype(np.float32)).to(cuda)
+    big = torch.tensor([2.0 * float(v1.double().abs().sum())], dtype=torch.float64, device=cuda)
+    w1, lam1 = _noalloc(v1, big, cuda)
+    torch.cuda.synchronize()
+    assert torch.equal(w1, v1) and float(lam1) == 0.0
+    v2 = (rng.standard_normal(400_000) * 0.5).astype(np.float32)
+    v2[rng.random(v2.size) < 0.1] = 0.0
+    b = 0.25 * float(np.abs(v2.astype(np.float64)).sum())
+    w2, lam2 = _noalloc(torch.from_numpy(v2).to(cuda),
+                        torch.tensor([b], dtype=torch.float64, device=cuda), cuda)
+    torch.cuda.synchronize()
+    lam_ref = O.l1ball_lambda_exact(v2, b)
+    assert abs(float(lam2) - lam_ref) <= 1e-6 * lam_ref
+    ref = np.sign(v2) * np.maximum(np.abs(v2.astype(np.float64)) - lam_ref, 0.0)
+    assert float(np.abs(w2.cpu().numpy() - ref).max()) <= TOL * max(1.0, float(np.abs(ref).max()))
+
+
 def test_noalloc_rejects_oversized_input(cuda):
     v = torch.zeros(8, device=cuda)
     w = torch.empty_like(v)
