@@ -701,6 +701,16 @@ def run_train(args):
     launches = L.dtv_launch_count() - n0
     plan = proj.plan(dev, 2)
     fp_units = 2 * plan.fp_samples()  # per forward projection of the batch
+    # the exact adjoint alone: each sample adds two 16-byte vector reductions
+    # into L2-resident cell records, so its bound is the L2's rate of those
+    # reductions, measured here with a kernel that does nothing else
+    adj_in = torch.rand(plan.sino_shape(2), device=dev)
+    adj_out = torch.empty(plan.vol_shape(2), device=dev)
+    plan.adjoint(adj_in, out=adj_out)
+    t_adj = time_steps(lambda: plan.adjoint(adj_in, out=adj_out), 10, stream) / 10
+    v4_contig = dtvb200._lib.measure_atomic_v4_rate(72 << 16, 0)
+    v4_scatter = dtvb200._lib.measure_atomic_v4_rate(72 << 16, 1)
+    adj_rate = 2 * fp_units / t_adj
     # per training step: each stage runs FP + A^T forward, recomputes them under
     # checkpointing, and backpropagates through both (FP + A^T again)
     units = stages * 3 * 2 * fp_units
@@ -713,6 +723,18 @@ def run_train(args):
         "config": {"workload": "10-stage unrolled PDHG net, batch 2 x 128^3, 48 views of 192^2",
                    "checkpointing": "per stage"},
         "projector_gsamples_per_s": units * args.steps / secs / 1e9,
+        "roofline": {
+            "bound": "l2-atomic", "kernel": "exact adjoint (cell-record scatter + gather)",
+            "unit": "float4 reductions/s", "achieved": adj_rate, "peak": v4_contig,
+            "frac": adj_rate / v4_contig,
+            "peak_source": ("measured in this run (dtv_measure_atomic_v4_rate: each warp's 32 "
+                            "lanes on 32 consecutive 16-byte records, 75 MB of records)"),
+            "scattered_peak": v4_scatter,
+            "adjoint_ms": t_adj * 1e3,
+            "reductions_per_launch": 2 * fp_units,
+            "note": ("two reductions per forward-projector sample of the batch (samples whose "
+                     "cell lies wholly in the zero border add none, so achieved is an upper "
+                     "bound)")},
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }

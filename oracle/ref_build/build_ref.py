@@ -53,7 +53,10 @@ def build(ref_root: str, verbose: bool = False) -> list:
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-root", default="/root/reference")
+    ap.add_argument("--ref-root", default=os.environ.get(
+        "DTV_REFERENCE_ROOT", os.path.join(os.path.dirname(REPO), "reference")),
+        help="reference checkout (default: $DTV_REFERENCE_ROOT, else ../reference beside "
+             "this repository)")
     ap.add_argument("-v", "--verbose", action="store_true")
     a = ap.parse_args()
     os.environ.setdefault("TORCH_CUDA_ARCH_LIST", "10.0a")

@@ -66,7 +66,8 @@ def _stub_layers():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-root", default="/root/reference")
+    ap.add_argument("--ref-root", default=os.environ.get(
+        "DTV_REFERENCE_ROOT", os.path.join(os.path.dirname(REPO), "reference")))
     ap.add_argument("--out", default=os.path.join(HERE, "ref_utils.npz"))
     a = ap.parse_args()
     sys.path.insert(0, a.ref_root)
