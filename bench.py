@@ -267,13 +267,16 @@ def cpu_baseline(c, truth_np, views_per_step=2, steps=1, warmup=0):
     return total_units / elapsed / 1e9, cores, sample, elapsed
 
 
-def fp64_check(c, dev, sampler, prm, plan, truth, sino_clean, f_dtypes):
+def fp64_check(c, dev, sampler, plan, truth, sino_clean, variants):
     """Checker leg, outside every timed region: relative RMSE against the FP64
     oracle of (1) the workload's forward projection of the phantom and (2) its
     FDK backprojection, both at full size on 16 of the views, and (3) the
     100-iteration reconstruction, on a same-FOV downsample by CHECK_DOWNSAMPLE
     (edge, detector and views per FOV scaled together; 64 views kept), with the
-    same sampler, storage, step-size rule and noise model as the timed run."""
+    same sampler, storage, step-size rule and noise model as the timed run.
+    ``variants``: (name, f_dtype, correct_every) reconstructions to check;
+    correct_every > 0 corrects the sampler's operators with an "exact" plan
+    every that many iterations (DTVCP's ``exact``), 0 runs it uncorrected."""
     import numpy as np
     import torch
 
@@ -319,10 +322,15 @@ def fp64_check(c, dev, sampler, prm, plan, truth, sino_clean, f_dtypes):
     ref = O.dtvcp_run(fpo, bpo, np.zeros((1, 1) + og_d.vol_shape), sino_np, dvs, c["iters"],
                       prm_d["sigma"], prm_d["tau"], prm_d["mu"], prm_d["v"], quirk=prm_d["quirk"])
     recon = {}
-    for name, fdt in f_dtypes:
+    exact_d = None
+    for name, fdt, every in variants:
         pl = plan_d if fdt == torch.float32 or sampler != "pairs" else \
             dtvb200.Plan(geo_d, max_batch=1, sampler=sampler, stage_f16=True, device=dev)
-        alg = dtvb200.DTVCP(pl, c["iters"], t_refresh=10, use_graph=True, f_dtype=fdt, **prm_d)
+        if every and exact_d is None:
+            exact_d = dtvb200.Plan(geo_d, max_batch=1, sampler="exact", device=dev)
+        alg = dtvb200.DTVCP(pl, c["iters"], t_refresh=10, use_graph=True, f_dtype=fdt,
+                            exact=exact_d if every else None, correct_every=max(every, 1),
+                            **prm_d)
         recon[name] = rel(alg.run(torch.zeros(pl.vol_shape(1), device=dev), sino_d).cpu().numpy(),
                           ref)
     return {
@@ -448,7 +456,12 @@ def run_ours(args):
     sino_clean = plan.forward(truth)
     sino = poisson_noise(sino_clean, c["i0"], seed=c["seed"] + rank)
     prm = dtv_params(plan, dev)
-    alg = dtvb200.DTVCP(plan, c["iters"], t_refresh=10, use_graph=True, **prm)
+    # texture-filtered samplers are corrected by the exact-weight plan every
+    # K iterations, which keeps the reconstruction within 1e-3 of FP64
+    K = args.correct_every if args.sampler in ("pairs", "tex", "tma") else 0
+    xplan = dtvb200.Plan(geo, max_batch=1, sampler="exact", device=dev) if K else None
+    corr = dict(exact=xplan, correct_every=max(K, 1))
+    alg = dtvb200.DTVCP(plan, c["iters"], t_refresh=10, use_graph=True, **corr, **prm)
     img = torch.zeros(plan.vol_shape(1), device=dev)
     stream = torch.cuda.current_stream(dev)
 
@@ -486,6 +499,12 @@ def run_ours(args):
 
     # ---- per-operator profile (eager pass with events on the launching stream)
     t_fp, t_bp, t_up = op_profile(plan, alg, img, sino, dev)
+    t_xfp = t_xbp = 0.0
+    if xplan is not None:  # the exact operators of each correction, timed alone
+        xs = torch.empty(plan.sino_shape(1), device=dev)
+        xv = torch.empty(plan.vol_shape(1), device=dev)
+        t_xfp = time_steps(lambda: xplan.forward(img + 0.5, out=xs), 5, stream) / 5 * 1e3
+        t_xbp = time_steps(lambda: xplan.backward(sino, out=xv), 5, stream) / 5 * 1e3
     n_views, P = c["n_views"], c["n_views"] * c["nu"] * c["nv"]
     fp_bytes = n_views * V * 4 + P * 4  # one volume pass per view + sinogram write (FP32)
     peaks = {}
@@ -502,7 +521,7 @@ def run_ours(args):
         ref_f = alg.run(img, sino)
         plan16 = dtvb200.Plan(geo, max_batch=1, sampler=args.sampler, stage_f16=True, device=dev)
         alg16 = dtvb200.DTVCP(plan16, c["iters"], t_refresh=10, use_graph=True,
-                              f_dtype=torch.float16, **prm)
+                              f_dtype=torch.float16, **corr, **prm)
         alg16.run(img, sino)
         s16 = time_steps(lambda: alg16.run(img, sino), args.steps, stream)
         f16 = alg16.run(img, sino)
@@ -527,8 +546,10 @@ def run_ours(args):
 
     cpu = check = ref_cuda = None
     if rank == 0 and ws == 1 and not args.no_check:
-        check = fp64_check(c, dev, args.sampler, prm, plan, truth, sino_clean,
-                           [("fp32_f", torch.float32), ("fp16_fbar", torch.float16)])
+        variants = [("fp32_f", torch.float32, K), ("fp16_fbar", torch.float16, K)]
+        if K:
+            variants.append(("fp32_f_uncorrected", torch.float32, 0))
+        check = fp64_check(c, dev, args.sampler, plan, truth, sino_clean, variants)
         ref_cuda = reference_cuda_baseline(c, dev, truth)
     if rank == 0 and ws == 1 and not args.no_cpu:
         # 48 of the 64 views: about 10-20 s of FP64 work on the host cores
@@ -547,10 +568,15 @@ def run_ours(args):
                    "l2": "working set > L2 (volume, 4 dual volumes, sinograms ~0.5 GB)",
                    "storage": ("f, duals, sinograms FP32; the projected volume staged as "
                                "FP16 z-pairs; FP32 accumulation"),
+                   "correction": (f"operators corrected by the exact-weight plan every {K} "
+                                  f"iterations (DTVCP exact=)" if K else None),
                    "inputs": "seeded ellipsoid phantom, Poisson noise"},
         "recon_per_s": recon_s,
         "samples_per_recon": units,
-        "per_iteration_ms": {"forward": t_fp, "backward": t_bp, "updates": t_up},
+        "per_iteration_ms": {"total": secs / args.steps / c["iters"] * 1e3, "forward": t_fp,
+                             "backward": t_bp, "updates": t_up,
+                             "exact_forward": t_xfp or None, "exact_backward": t_xbp or None,
+                             "correct_every": K or None},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak,
                      "traffic": FP_NCU.get(args.sampler, {}).get("traffic"),
@@ -948,6 +974,9 @@ def main():
     ap.add_argument("--small", action="store_true", help="64^3 smoke-size workload")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--correct-every", type=int, default=10, metavar="K",
+                    help="refresh the exact-weight correction of a texture-filtered sampler "
+                         "every K DTV iterations (0: uncorrected)")
     ap.add_argument("--no-check", action="store_true",
                     help="skip the FP64 error check and the reference-CUDA baseline")
     ap.add_argument("--workload", choices=["sparse_dtv", "batch16", "train", "fista64",

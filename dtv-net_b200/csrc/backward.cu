@@ -10,6 +10,7 @@
 // kernel; the projective map of each view (FP64-derived, see geometry.cu)
 // gives the detector coordinates with one reciprocal per voxel-view.
 #include <algorithm>
+#include <type_traits>
 #include <string.h>
 
 #include "common.cuh"
@@ -55,6 +56,27 @@ struct SoftBil {
   }
 };
 
+// The same bilinear sample from 16-byte records of the padded view (exact
+// plans): record (U, V) = (s(U, V), s(U+1, V), s(U, V+1), s(U+1, V+1)) at
+// padded indices, one 128-bit load per voxel-view.
+struct QuadBil {
+  const float4* q;  // records of the view
+  int pu;
+  float mu, mv;
+  __device__ __forceinline__ float operator()(float u, float v) const {
+    const float fu = floorf(u), fv = floorf(v);
+    const float au = u - fu, av = v - fv;
+    const int iu = (int)fminf(fmaxf(fu, -2.f), mu) + kPad;
+    const int iv = (int)fminf(fmaxf(fv, -2.f), mv) + kPad;
+    const float4 r = __ldg(q + iv * pu + iu);
+    const float c0 = fmaf(au, r.y - r.x, r.x), c1 = fmaf(au, r.w - r.z, r.z);
+    return fmaf(av, c1 - c0, c0);
+  }
+};
+
+// Where the backprojector's detector values come from.
+enum BPSource { kSrcSoft = 0, kSrcTex = 1, kSrcQuad = 2 };
+
 // kZAff: every view's u and h are independent of z (a detector parallel to the
 // rotation axis, as in the circular orbits), so per column and view the kernel
 // computes u, 1/h and the weight once and each voxel costs one FMA for v, one
@@ -72,7 +94,7 @@ struct TableMaps {
 
 // One block's columns: tile `tile` of 16x16 (x, y) columns, z-chunk `zc` of ZC
 // voxels, views n0 .. n0 + n_chunk - 1.
-template <bool kTex, bool kZAff, int ZC, class Maps>
+template <int kSrc, bool kZAff, int ZC, class Maps>
 __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps, int n0, int n_chunk,
                                            const float* __restrict__ spad, cudaTextureObject_t tex,
                                            float* __restrict__ out, int accumulate, int tile,
@@ -123,7 +145,13 @@ __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps,
     const float bu = fmaf(m0, fi, fmaf(m1, fj, m3));
     const float bv = fmaf(m4, fi, fmaf(m5, fj, m7));
     const float bh = fmaf(m8, fi, fmaf(m9, fj, m11));
-    SoftBil smp{spad + (int64_t)n * bp.sino_pad_elems, pu, mu, mv};
+    using Smp = typename std::conditional<kSrc == kSrcQuad, QuadBil, SoftBil>::type;
+    Smp smp;
+    if constexpr (kSrc == kSrcQuad)
+      smp = QuadBil{reinterpret_cast<const float4*>(spad) + (int64_t)n * bp.sino_pad_elems, pu,
+                    mu, mv};
+    else
+      smp = SoftBil{spad + (int64_t)n * bp.sino_pad_elems, pu, mu, mv};
     if constexpr (kZAff) {
       const float rh = __frcp_rn(bh);
       // v from the absolute slice index: the same bits for every z-chunking
@@ -139,7 +167,7 @@ __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps,
         float wz = wgt;
         if (bp.extent && (v + 0.5f < -1.f || v + 0.5f > bp.ny + 1.f)) wz = 0.f;
         float val;
-        if constexpr (kTex) val = tex2DLayered<float>(tex, u + 0.5f, v + 0.5f, n);
+        if constexpr (kSrc == kSrcTex) val = tex2DLayered<float>(tex, u + 0.5f, v + 0.5f, n);
         else val = smp(u, v);
         acc[z] = fmaf(val, wz, acc[z]);
       }
@@ -159,7 +187,7 @@ __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps,
           if (tx < -1.f || tx > bp.nx + 1.f || ty < -1.f || ty > bp.ny + 1.f) wgt = 0.f;
         }
         float val;
-        if constexpr (kTex) val = tex2DLayered<float>(tex, u + 0.5f, v + 0.5f, n);
+        if constexpr (kSrc == kSrcTex) val = tex2DLayered<float>(tex, u + 0.5f, v + 0.5f, n);
         else val = smp(u, v);
         acc[z] = fmaf(val, wgt, acc[z]);
       }
@@ -177,14 +205,33 @@ __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps,
   }
 }
 
-template <bool kTex, bool kZAff, int ZC>
+template <int kSrc, bool kZAff, int ZC>
 __global__ void __launch_bounds__(kBPThreads) bp_kernel(BPParams bp, const __grid_constant__ BPMaps maps,
                                                         int n0, int n_chunk,
                                                         const float* __restrict__ spad,
                                                         cudaTextureObject_t tex,
                                                         float* __restrict__ out, int accumulate) {
-  bp_columns<kTex, kZAff, ZC>(bp, ParamMaps{&maps}, n0, n_chunk, spad, tex, out, accumulate,
+  bp_columns<kSrc, kZAff, ZC>(bp, ParamMaps{&maps}, n0, n_chunk, spad, tex, out, accumulate,
                               (int)blockIdx.x, (int)blockIdx.y);
+}
+
+// Records of the exact backprojector: record (U, V) of view n from the four
+// detector values (u, v) = (U - 2 .. U - 1, V - 2 .. V - 1), zero outside the
+// view. Only records that reach the view (U in [1, nu+1], V in [1, nv+1]) are
+// written; the rest keep the plan's initial zeros.
+__global__ void stage_sino_quad_kernel(const float* __restrict__ in, float4* __restrict__ out,
+                                       int nu, int nv, int n_views) {
+  const int U = blockIdx.x * 32 + (threadIdx.x & 31) + 1;
+  const int V = blockIdx.y * 8 + (threadIdx.x >> 5) + 1;
+  const int n = blockIdx.z;
+  if (U > nu + 1 || V > nv + 1 || n >= n_views) return;
+  const float* s = in + (int64_t)n * nu * nv;
+  const int u = U - kPad, v = V - kPad;
+  auto at = [&](int uu, int vv) {
+    return (uu >= 0 && uu < nu && vv >= 0 && vv < nv) ? __ldg(s + (int64_t)vv * nu + uu) : 0.f;
+  };
+  out[(int64_t)n * (nu + 2 * kPad) * (nv + 2 * kPad) + (int64_t)V * (nu + 2 * kPad) + U] =
+      make_float4(at(u, v), at(u + 1, v), at(u, v + 1), at(u + 1, v + 1));
 }
 
 __global__ void stage_sino_pad_kernel(const float* __restrict__ in, float* __restrict__ out, int nu,
@@ -210,25 +257,31 @@ static int bp_zc(BlocksFor blocks_for) {
   return 2;
 }
 
-template <bool kTex, bool kZAff>
+template <int kSrc, bool kZAff>
 static void launch_bp_zc(int zc, dim3 grid, cudaStream_t st, const BPParams& bp,
                          const BPMaps& maps, int n0, int cnt, const float* sp,
                          cudaTextureObject_t tx, float* ob, int acc) {
   if (zc == 8)
-    bp_kernel<kTex, kZAff, 8><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, ob, acc);
+    bp_kernel<kSrc, kZAff, 8><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, ob, acc);
   else if (zc == 4)
-    bp_kernel<kTex, kZAff, 4><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, ob, acc);
+    bp_kernel<kSrc, kZAff, 4><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, ob, acc);
   else
-    bp_kernel<kTex, kZAff, 2><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, ob, acc);
+    bp_kernel<kSrc, kZAff, 2><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, ob, acc);
 }
 
-static void launch_bp(bool tex, bool zaff, int zc, dim3 grid, cudaStream_t st, const BPParams& bp,
+static void launch_bp(int src, bool zaff, int zc, dim3 grid, cudaStream_t st, const BPParams& bp,
                       const BPMaps& maps, int n0, int cnt, const float* sp, cudaTextureObject_t tx,
                       float* ob, int acc) {
-  if (tex && zaff) launch_bp_zc<true, true>(zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
-  else if (tex) launch_bp_zc<true, false>(zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
-  else if (zaff) launch_bp_zc<false, true>(zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
-  else launch_bp_zc<false, false>(zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
+  if (src == kSrcTex) {
+    if (zaff) launch_bp_zc<kSrcTex, true>(zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
+    else launch_bp_zc<kSrcTex, false>(zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
+  } else if (src == kSrcQuad) {
+    if (zaff) launch_bp_zc<kSrcQuad, true>(zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
+    else launch_bp_zc<kSrcQuad, false>(zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
+  } else {
+    if (zaff) launch_bp_zc<kSrcSoft, true>(zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
+    else launch_bp_zc<kSrcSoft, false>(zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
+  }
 }
 
 int backward_impl(Plan* p, const float* sino, int batch, float* out, int accumulate,
@@ -243,6 +296,7 @@ int backward_impl(Plan* p, const float* sino, int batch, float* out, int accumul
   bp.sino_pad_elems = (int64_t)(gp.nu + 2 * kPad) * (gp.nv + 2 * kPad);
   bp.warp = p->bp_warp;
   const bool tex = p->sino_tex != nullptr;  // allocated for the texture plans
+  const bool quad = p->d_sino_quad != nullptr;  // the exact plans
   const int tiles = ((gp.nx + kBPTile - 1) / kBPTile) * ((gp.ny + kBPTile - 1) / kBPTile);
   const int zc = bp_zc([&](int c) { return (int64_t)tiles * ((gp.nz + c - 1) / c); });
   dim3 grid(tiles, (gp.nz + zc - 1) / zc);
@@ -258,6 +312,11 @@ int backward_impl(Plan* p, const float* sino, int batch, float* out, int accumul
       cp.extent = make_cudaExtent(gp.nu, gp.nv, gp.n_views);
       cp.kind = cudaMemcpyDeviceToDevice;
       DTV_CUDA_TRY(cudaMemcpy3DAsync(&cp, st));
+    } else if (quad) {
+      dim3 qg((gp.nu + 1 + 31) / 32, (gp.nv + 1 + 7) / 8, gp.n_views);
+      stage_sino_quad_kernel<<<qg, 256, 0, st>>>(sino + b * per_item, p->d_sino_quad, gp.nu,
+                                                 gp.nv, gp.n_views); note_launch();
+      DTV_LAUNCH_CHECK();
     } else {
       stage_sino_pad_kernel<<<(int)std::min<int64_t>((per_item + 255) / 256, 148 * 16), 256, 0,
                               st>>>(sino + b * per_item, p->d_sino_pad, gp.nu, gp.nv, gp.n_views); note_launch();
@@ -265,13 +324,15 @@ int backward_impl(Plan* p, const float* sino, int batch, float* out, int accumul
     }
     float* ob = out + (int64_t)b * gp.nx * gp.ny * gp.nz;
     const cudaTextureObject_t tx = tex ? p->sino_tex[0] : 0;
-    const float* sp = tex ? nullptr : p->d_sino_pad;
+    const float* sp = tex ? nullptr
+                          : quad ? reinterpret_cast<const float*>(p->d_sino_quad) : p->d_sino_pad;
+    const int src = tex ? kSrcTex : quad ? kSrcQuad : kSrcSoft;
     // views in chunks of kBPParamViews; later chunks accumulate
     for (int n0 = 0; n0 < gp.n_views; n0 += kBPParamViews) {
       const int cnt = std::min(kBPParamViews, gp.n_views - n0);
       for (int j = 0; j < cnt; ++j) memcpy(maps.m[j], p->h_bpv[n0 + j].m, sizeof(maps.m[j]));
       const int acc = n0 > 0 ? 1 : accumulate;
-      launch_bp(tex, p->bp_zaffine != 0, zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
+      launch_bp(src, p->bp_zaffine != 0, zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
       note_launch();
       DTV_LAUNCH_CHECK();
     }
@@ -308,10 +369,10 @@ __global__ void __launch_bounds__(kBPThreads) bp_many_kernel(const __grid_consta
   const int local = (int)blockIdx.x - it.block0;
   const int tile = local % it.tiles, zc = local / it.tiles;
   if (it.zaffine)
-    bp_columns<true, true, ZC>(it.bp, TableMaps{it.views}, 0, it.bp.n_views, nullptr, it.tex,
+    bp_columns<kSrcTex, true, ZC>(it.bp, TableMaps{it.views}, 0, it.bp.n_views, nullptr, it.tex,
                                it.out, accumulate, tile, zc);
   else
-    bp_columns<true, false, ZC>(it.bp, TableMaps{it.views}, 0, it.bp.n_views, nullptr, it.tex,
+    bp_columns<kSrcTex, false, ZC>(it.bp, TableMaps{it.views}, 0, it.bp.n_views, nullptr, it.tex,
                                 it.out, accumulate, tile, zc);
 }
 

@@ -58,6 +58,20 @@ __device__ __forceinline__ void store_from_float(__nv_bfloat16* p, int64_t i, fl
   p[i] = __float2bfloat16_rn(v);
 }
 
+// The half2 held in a 32-bit word (low half first, as surface and linear
+// z-pair copies store it).
+__device__ __forceinline__ __half2 u32_as_half2(unsigned int w) {
+  return __halves2half2(__ushort_as_half((unsigned short)(w & 0xFFFFu)),
+                        __ushort_as_half((unsigned short)(w >> 16)));
+}
+
+// Record of padded column (X, Y) = (x + 2, y + 2) and z-pair layer L in the
+// 2 x 2 x 2-brick order of the exact sampler's records.
+__device__ __forceinline__ int pair_quad_index(int X, int Y, int L, int bx, int by) {
+  return ((((L >> 1) * by + (Y >> 1)) * bx + (X >> 1)) << 3) | ((L & 1) << 2) | ((Y & 1) << 1) |
+         (X & 1);
+}
+
 inline int dtype_size(int dt) { return dt == DTV_F32 ? 4 : 2; }
 inline bool dtype_ok(int dt) { return dt == DTV_F32 || dt == DTV_F16 || dt == DTV_BF16; }
 
@@ -118,6 +132,8 @@ struct Plan {
   int64_t pad_elems;  // elements of one padded volume
   // soft bilinear staging: zero-padded sinogram of one batch item
   float* d_sino_pad;
+  // exact plans: 16-byte records (2x2 detector values) of the padded sinogram
+  float4* d_sino_quad;
   // texture sampler (DTV_PLAN_TEX): one 3-D array per batch item for the
   // volume, one layered array for a sinogram
   cudaArray_t* vol_arrays;
@@ -139,6 +155,13 @@ struct Plan {
   // (boxes for chunks along x and along y)
   unsigned int* d_pair_lin;
   int pair_pitch;
+  // exact z-pair sampler (DTV_PLAN_PAIRS_EXACT): per batch item, 16-byte
+  // records (x, y, L) of the four x/y corner words of a z-pair cell over the
+  // grid padded by two zero texels in x and y, in 2 x 2 x 2 bricks of
+  // 128 bytes (pair_quad_index)
+  uint4* d_pair_quad;
+  int64_t pair_quad_elems;  // records per batch item
+  int quad_bx, quad_by;     // bricks along x and y
   int fp_tex_share;          // DTV_TUNE_FP_TEX_SHARE
   alignas(64) unsigned char tmap[2][128];
   int* d_status;             // device error bits

@@ -69,6 +69,35 @@ struct QuadSampler {
   }
 };
 
+// Exact trilinear sample of the FP16 z pairs (DTV_PLAN_PAIRS_EXACT): one
+// 16-byte record holds the four x/y corner words of the sample's cell, word =
+// (f[L-2], f[L-1]) at layer L = floor(z) + 2, so a sample is one 128-bit load
+// through L1 and FP32 x/y/z weights. Positions arrive in voxel index
+// coordinates; the ray set-up keeps them within one step of (-1, n), and the
+// clamps keep every record inside the zero-padded grid whatever the rounding.
+struct PairQuadSampler {
+  const uint4* rec;    // records of this batch item
+  int bx, by;          // bricks along x and y
+  float mx, my, lmax;  // nx, ny, nz + 2
+  __device__ __forceinline__ float operator()(float x, float y, float z) const {
+    const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
+    const float ax = x - fx, ay = y - fy, az = z - fz;
+    const int X = (int)fminf(fmaxf(fx, -2.f), mx) + 2;
+    const int Y = (int)fminf(fmaxf(fy, -2.f), my) + 2;
+    const int L = (int)fminf(fmaxf(fz + 2.f, 0.f), lmax);
+    const uint4 r = __ldg(rec + pair_quad_index(X, Y, L, bx, by));
+    const float2 c00 = __half22float2(u32_as_half2(r.x));
+    const float2 c10 = __half22float2(u32_as_half2(r.y));
+    const float2 c01 = __half22float2(u32_as_half2(r.z));
+    const float2 c11 = __half22float2(u32_as_half2(r.w));
+    // lerps in the order of SoftSampler: x, then y, then z
+    const float a0 = fmaf(ax, c10.x - c00.x, c00.x), a1 = fmaf(ax, c11.x - c01.x, c01.x);
+    const float b0 = fmaf(ax, c10.y - c00.y, c00.y), b1 = fmaf(ax, c11.y - c01.y, c01.y);
+    const float lo = fmaf(ay, a1 - a0, a0), hi = fmaf(ay, b1 - b0, b0);
+    return fmaf(az, hi - lo, lo);
+  }
+};
+
 // Texture coordinates: the ray set-up already added the 1/2 texel offset.
 struct TexSampler {
   cudaTextureObject_t tex;
@@ -189,6 +218,41 @@ __global__ void __launch_bounds__(kFPThreads) fp_pair_kernel(RayParams rp, const
   if (o.abs_sum) block_add_double((double)fabsf(res), o.abs_sum);
 }
 
+__global__ void __launch_bounds__(kFPThreads) fp_pairx_kernel(RayParams rp,
+                                                              const FPView* __restrict__ views,
+                                                              const uint4* __restrict__ rec,
+                                                              int64_t rec_elems, int bx, int by,
+                                                              FPOut o) {
+  int u, v, n;
+  tile_pixel(rp, u, v, n);
+  const int b = blockIdx.z;
+  float res = 0.f;
+  if (u < rp.nu && v < rp.nv) {
+    const RaySetup rs = setup_ray(rp, views[n], u, v);
+    PairQuadSampler smp;
+    smp.rec = rec + b * rec_elems;
+    smp.bx = bx;
+    smp.by = by;
+    smp.mx = (float)rp.nx;
+    smp.my = (float)rp.ny;
+    smp.lmax = (float)(rp.nz + 2);
+    const float val = rs.count > 0 ? ray_sum(smp, rs) * rp.scale : 0.f;
+    fp_store(rp, o, n, b, u, v, val, res);
+  }
+  if (o.abs_sum) block_add_double((double)fabsf(res), o.abs_sum);
+}
+
+// Writes the exact sampler's records of one volume: record (X, Y, L) =
+// words (X, Y), (X+1, Y), (X, Y+1), (X+1, Y+1) of z-pair layer L, word =
+// half2(f[L-2], f[L-1]) at padded column (X, Y) = (x + 2, y + 2), zero outside
+// the volume. Only records that reach the volume are written (X in [1, nx+1],
+// Y in [1, ny+1], L in [1, nz+1]); the others keep the plan's initial zeros.
+// A thread owns one record column and kStageLayers layers of it.
+template <class Tin>
+__global__ void __launch_bounds__(256) stage_pair_quads_kernel(const Tin* __restrict__ in,
+                                                               uint4* __restrict__ rec, int nx,
+                                                               int ny, int nz, int bx, int by);
+
 // Writes the z-pair layers of one volume: layer L = (f[L-2], f[L-1]), zero
 // outside [0, nz), to the layered texture and, when `lin` is set, to the
 // linear [nz+3][ny][pitch] copy. A thread owns one (x, y) column and a run of
@@ -199,7 +263,8 @@ template <class Tin>
 __global__ void __launch_bounds__(256) stage_pairs_kernel(const Tin* __restrict__ in,
                                                           cudaSurfaceObject_t surf,
                                                           unsigned int* __restrict__ lin, int pitch,
-                                                          int nx, int ny, int nz) {
+                                                          int64_t lin_plane, int nx, int ny,
+                                                          int nz) {
   const int x = blockIdx.x * 32 + (threadIdx.x & 31);
   const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
   if (x >= nx || y >= ny) return;
@@ -217,9 +282,44 @@ __global__ void __launch_bounds__(256) stage_pairs_kernel(const Tin* __restrict_
     const __half cur = member(L - 1);  // the new member f[L-1]
     const unsigned int bits = (unsigned int)__half_as_ushort(prev) |
                               ((unsigned int)__half_as_ushort(cur) << 16);
-    surf2DLayeredwrite(bits, surf, x * 4, y, L);
-    if (lin) lin[((int64_t)L * ny + y) * pitch + x] = bits;
+    if (surf) surf2DLayeredwrite(bits, surf, x * 4, y, L);
+    if (lin) lin[(int64_t)L * lin_plane + (int64_t)y * pitch + x] = bits;
     prev = cur;
+  }
+}
+
+template <class Tin>
+__global__ void __launch_bounds__(256) stage_pair_quads_kernel(const Tin* __restrict__ in,
+                                                               uint4* __restrict__ rec, int nx,
+                                                               int ny, int nz, int bx, int by) {
+  const int X = blockIdx.x * 32 + (threadIdx.x & 31) + 1;
+  const int Y = blockIdx.y * 8 + (threadIdx.x >> 5) + 1;
+  if (X > nx + 1 || Y > ny + 1) return;
+  const int L0 = 1 + blockIdx.z * kStageLayers;
+  const int L1 = min(L0 + kStageLayers, nz + 2);
+  const int64_t plane = (int64_t)nx * ny;
+  const int x = X - 2, y = Y - 2;
+  // the four columns of the record: (x, y), (x+1, y), (x, y+1), (x+1, y+1)
+  const bool in_c[4] = {x >= 0 && y >= 0, x + 1 < nx && y >= 0, x >= 0 && y + 1 < ny,
+                        x + 1 < nx && y + 1 < ny};
+  const int64_t off[4] = {(int64_t)y * nx + x, (int64_t)y * nx + x + 1,
+                          (int64_t)(y + 1) * nx + x, (int64_t)(y + 1) * nx + x + 1};
+  auto member = [&](int c, int z) {
+    return (in_c[c] && z >= 0 && z < nz) ? __float2half_rn(load_as_float(in + off[c], z * plane))
+                                         : __float2half_rn(0.f);
+  };
+  __half prev[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) prev[c] = member(c, L0 - 2);
+  for (int L = L0; L < L1; ++L) {
+    unsigned int wd[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const __half cur = member(c, L - 1);
+      wd[c] = (unsigned int)__half_as_ushort(prev[c]) | ((unsigned int)__half_as_ushort(cur) << 16);
+      prev[c] = cur;
+    }
+    rec[pair_quad_index(X, Y, L, bx, by)] = make_uint4(wd[0], wd[1], wd[2], wd[3]);
   }
 }
 
@@ -335,10 +435,19 @@ static int stage_volume_pairs(Plan* p, const Tin* vol, int batch, cudaStream_t s
   const int64_t vox = (int64_t)g.nx * g.ny * g.nz;
   dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + 3 + kStageLayers - 1) / kStageLayers);
   for (int b = 0; b < batch; ++b) {
-    unsigned int* lin =
-        p->d_pair_lin ? p->d_pair_lin + (int64_t)b * p->pair_pitch * g.ny * (g.nz + 3) : nullptr;
-    stage_pairs_kernel<Tin><<<grid, 256, 0, st>>>(vol + b * vox, p->pair_surf[b], lin,
-                                                  p->pair_pitch, g.nx, g.ny, g.nz); note_launch();
+    if (p->d_pair_quad) {  // exact sampler: its records only
+      dim3 qg((g.nx + 1 + 31) / 32, (g.ny + 1 + 7) / 8, (g.nz + 1 + kStageLayers - 1) / kStageLayers);
+      stage_pair_quads_kernel<Tin><<<qg, 256, 0, st>>>(vol + b * vox,
+                                                       p->d_pair_quad + b * p->pair_quad_elems,
+                                                       g.nx, g.ny, g.nz, p->quad_bx,
+                                                       p->quad_by); note_launch();
+    } else {
+      unsigned int* lin =
+          p->d_pair_lin ? p->d_pair_lin + (int64_t)b * p->pair_pitch * g.ny * (g.nz + 3) : nullptr;
+      stage_pairs_kernel<Tin><<<grid, 256, 0, st>>>(vol + b * vox, p->pair_surf[b], lin,
+                                                    p->pair_pitch, (int64_t)p->pair_pitch * g.ny,
+                                                    g.nx, g.ny, g.nz); note_launch();
+    }
     DTV_LAUNCH_CHECK();
   }
   return DTV_OK;
@@ -349,7 +458,7 @@ int forward_impl(Plan* p, const void* vol, int vol_dtype, int batch, float* out,
   const GeomParams& gp = p->gp;
   int rc;
   const bool tex = (p->flags & DTV_PLAN_TEX) != 0;
-  const bool pairs = (p->flags & DTV_PLAN_TEX_PAIRS) != 0;
+  const bool pairs = (p->flags & (DTV_PLAN_TEX_PAIRS | DTV_PLAN_PAIRS_EXACT)) != 0;
   switch (vol_dtype) {
     case DTV_F32:
       rc = pairs ? stage_volume_pairs(p, (const float*)vol, batch, st)
@@ -378,6 +487,9 @@ int forward_impl(Plan* p, const void* vol, int vol_dtype, int batch, float* out,
   dim3 grid(tiles, gp.n_views, batch);
   if (p->flags & DTV_PLAN_TMA) {
     return fp_tma_launch(p, rp, o, batch, st);
+  } else if (p->d_pair_quad) {
+    fp_pairx_kernel<<<grid, kFPThreads, 0, st>>>(rp, p->d_fpv, p->d_pair_quad, p->pair_quad_elems,
+                                                 p->quad_bx, p->quad_by, o); note_launch();
   } else if (pairs) {
     fp_pair_kernel<<<grid, kFPThreads, 0, st>>>(rp, p->d_fpv, p->pair_tex_dev, o); note_launch();
   } else if (tex) {

@@ -56,6 +56,7 @@ void free_plan(Plan* p) {
   cudaFree(p->d_rays);
   cudaFree(p->d_cells);
   cudaFree(p->d_pair_lin);
+  cudaFree(p->d_pair_quad);
   cudaFree(p->d_status);
   cudaFree(p->d_fpv);
   cudaFree(p->d_bpv);
@@ -63,6 +64,7 @@ void free_plan(Plan* p) {
   cudaFree(p->d_vol_pad);
   cudaFree(p->d_vol_quads);
   cudaFree(p->d_sino_pad);
+  cudaFree(p->d_sino_quad);
   delete p;
 }
 
@@ -89,9 +91,12 @@ int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Pla
   DTV_CHECK(!(flags & DTV_PLAN_TMA) || (flags & DTV_PLAN_TEX_PAIRS),
             "DTV_PLAN_TMA needs DTV_PLAN_TEX_PAIRS");
   DTV_CHECK((flags & ~(DTV_PLAN_TEX | DTV_PLAN_STAGE_F16 | DTV_PLAN_TEX_PAIRS | DTV_PLAN_ADJOINT |
-                       DTV_PLAN_TMA)) ==
+                       DTV_PLAN_TMA | DTV_PLAN_PAIRS_EXACT)) ==
                 0,
             "unknown plan flags 0x%x", flags);
+  DTV_CHECK(!((flags & DTV_PLAN_PAIRS_EXACT) &&
+              (flags & (DTV_PLAN_TEX | DTV_PLAN_TEX_PAIRS | DTV_PLAN_TMA))),
+            "DTV_PLAN_PAIRS_EXACT excludes DTV_PLAN_TEX, DTV_PLAN_TEX_PAIRS and DTV_PLAN_TMA");
   DTV_CHECK(!((flags & DTV_PLAN_TEX) && (flags & DTV_PLAN_TEX_PAIRS)),
             "DTV_PLAN_TEX and DTV_PLAN_TEX_PAIRS are exclusive");
   int ndev = 0;
@@ -147,7 +152,19 @@ int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Pla
   const size_t esz = p->stage_dtype == DTV_F16 ? 2 : 4;
   // Staged volumes of the software sampler (FP32: quad records, FP16: the
   // padded volume): zero border written once here, interiors by each call.
-  if (!(flags & (DTV_PLAN_TEX | DTV_PLAN_TEX_PAIRS))) {
+  if (flags & DTV_PLAN_PAIRS_EXACT) {
+    p->quad_bx = (gp.nx + 4 + 1) / 2;
+    p->quad_by = (gp.ny + 4 + 1) / 2;
+    const int64_t bl = (gp.nz + 3 + 1) / 2;
+    p->pair_quad_elems = (int64_t)p->quad_bx * p->quad_by * bl * 8;
+    if (p->pair_quad_elems >= (1LL << 31)) {
+      free_plan(p);
+      return fail(DTV_ERR_UNSUPPORTED, "volume too large for DTV_PLAN_PAIRS_EXACT");
+    }
+    const size_t bytes = sizeof(uint4) * p->pair_quad_elems * max_batch;
+    PLAN_CUDA(cudaMalloc(&p->d_pair_quad, bytes));
+    PLAN_CUDA(cudaMemset(p->d_pair_quad, 0, bytes));  // records beyond the volume stay zero
+  } else if (!(flags & (DTV_PLAN_TEX | DTV_PLAN_TEX_PAIRS))) {
     if (p->stage_dtype == DTV_F32) {
       PLAN_CUDA(cudaMalloc(&p->d_vol_quads, sizeof(float4) * p->pad_elems * max_batch));
       PLAN_CUDA(cudaMemset(p->d_vol_quads, 0, sizeof(float4) * p->pad_elems * max_batch));
@@ -159,6 +176,10 @@ int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Pla
   const int64_t sino_pad = (int64_t)(gp.nu + 2 * kPad) * (gp.nv + 2 * kPad) * gp.n_views;
   PLAN_CUDA(cudaMalloc(&p->d_sino_pad, sizeof(float) * sino_pad));
   PLAN_CUDA(cudaMemset(p->d_sino_pad, 0, sizeof(float) * sino_pad));
+  if (flags & DTV_PLAN_PAIRS_EXACT) {
+    PLAN_CUDA(cudaMalloc(&p->d_sino_quad, sizeof(float4) * sino_pad));
+    PLAN_CUDA(cudaMemset(p->d_sino_quad, 0, sizeof(float4) * sino_pad));
+  }
 
   if (flags & DTV_PLAN_TEX) {
     p->vol_arrays = (cudaArray_t*)calloc(max_batch, sizeof(cudaArray_t));
@@ -280,6 +301,7 @@ int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Pla
     const double voxels = (double)gp.nx * gp.ny * gp.nz;
     double staged;
     if (flags & DTV_PLAN_TEX_PAIRS) staged = (double)gp.nx * gp.ny * (gp.nz + 3) * 4.0;
+    else if (flags & DTV_PLAN_PAIRS_EXACT) staged = (double)p->pair_quad_elems * 16.0;
     else if (flags & DTV_PLAN_TEX) staged = voxels * (p->stage_dtype == DTV_F16 ? 2.0 : 4.0);
     else if (p->d_vol_quads) staged = (double)p->pad_elems * 16.0;
     else staged = (double)p->pad_elems * 2.0;

@@ -834,6 +834,29 @@ __global__ void axpy_l1_kernel(float* __restrict__ f, const float* __restrict__ 
   if (l1) block_sums_atomic<1>(acc, l1);
 }
 
+// out = a x + b y.
+__global__ void lincomb_kernel(const float* __restrict__ x, float a, const float* __restrict__ y,
+                               float b, float* __restrict__ out, int64_t n) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x)
+    out[t] = fmaf(a, __ldg(x + t), b * __ldg(y + t));
+}
+
+// The PDHG sinogram dual step from a finished projection:
+// w = (w + sigma (fp - g)) / (1 + sigma), abs_sum += sum |fp - g|.
+__global__ void sino_dual_kernel(float* __restrict__ w, const float* __restrict__ fp,
+                                 const float* __restrict__ g, float sigma, int64_t n,
+                                 double* abs_sum) {
+  double acc[1] = {0.0};
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const float res = __ldg(fp + t) - __ldg(g + t);
+    w[t] = (w[t] + sigma * res) / (1.f + sigma);
+    acc[0] += fabsf(res);
+  }
+  if (abs_sum) block_sums_atomic<1>(acc, abs_sum);
+}
+
 // sum += sum |a - b| (FP64 accumulation): ASD-POCS's TV-change measure.
 __global__ void l1_distance_kernel(const float* __restrict__ a, const float* __restrict__ b,
                                    double* sum, int64_t n) {
@@ -1126,6 +1149,22 @@ int dtv_tv_descent(const float* f_in, float* f_out, const int32_t size[3], int32
   if (rc) return rc;
   Dims d = make_dims(size, quirk, batch);
   tv_descent_kernel<<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(f_in, f_out, d, davg); note_launch();
+  DTV_LAUNCH_CHECK();
+  return DTV_OK;
+}
+
+int dtv_lincomb(const float* x, float a, const float* y, float b, float* out, int64_t n,
+                void* stream) {
+  DTV_CHECK(x && y && out && n > 0, "bad argument");
+  lincomb_kernel<<<blocks_for(n), 256, 0, as_stream(stream)>>>(x, a, y, b, out, n); note_launch();
+  DTV_LAUNCH_CHECK();
+  return DTV_OK;
+}
+
+int dtv_pdhg_sino_dual(float* w, const float* fp, const float* g, float sigma, int64_t n,
+                       double* abs_sum, void* stream) {
+  DTV_CHECK(w && fp && g && n > 0, "bad argument");
+  sino_dual_kernel<<<blocks_for(n), 256, 0, as_stream(stream)>>>(w, fp, g, sigma, n, abs_sum); note_launch();
   DTV_LAUNCH_CHECK();
   return DTV_OK;
 }

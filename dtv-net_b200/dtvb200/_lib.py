@@ -17,6 +17,7 @@ DTV_PHASE_STANDARD, DTV_PHASE_VECTOR, DTV_PHASE_BOX = 0, 1, 2
 DTV_PLAN_SOFT, DTV_PLAN_TEX, DTV_PLAN_STAGE_F16, DTV_PLAN_TEX_PAIRS = 0x0, 0x1, 0x2, 0x4
 DTV_PLAN_ADJOINT = 0x8
 DTV_PLAN_TMA = 0x10
+DTV_PLAN_PAIRS_EXACT = 0x20
 DTV_TUNE_FP_RAY_TILE = 1
 DTV_TUNE_FP_TEX_SHARE = 2
 DTV_TUNE_ADJOINT = 3
@@ -107,8 +108,11 @@ SIGNATURES = {
     "dtv_tv_descent": [_P, _P, _IP, _I, _I, _P, _P],
     "dtv_scale_scalar": [_P, _D, _P, _P],
     "dtv_l1_distance": [_P, _P, _L, _P, _P],
+    "dtv_lincomb": [_P, _F, _P, _F, _P, _L, _P],
+    "dtv_pdhg_sino_dual": [_P, _P, _P, _F, _L, _P, _P],
     "dtv_asd_adapt": [_P, _P, _F, _F, _P, _P],
     "dtv_measure_texture_fetch_rate": [_I, _DP],
+    "dtv_measure_texture_gather_rate": [_I, _DP],
     "dtv_measure_atomic_v4_rate": [_L, _I, _DP],
 }
 _RESTYPES = {
@@ -153,6 +157,13 @@ def measure_texture_fetch_rate(texel_bits: int = 32) -> float:
     """Bilinear texture fetches per second of the current device (benchmarks)."""
     out = ctypes.c_double()
     call("dtv_measure_texture_fetch_rate", texel_bits, ctypes.byref(out))
+    return out.value
+
+
+def measure_texture_gather_rate(gather: int = 1) -> float:
+    """Gathers (or bilinear fetches) per second from a tiled 2-D texture (benchmarks)."""
+    out = ctypes.c_double()
+    call("dtv_measure_texture_gather_rate", gather, ctypes.byref(out))
     return out.value
 
 

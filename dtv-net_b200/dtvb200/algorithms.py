@@ -139,16 +139,35 @@ class DTVCP(_Graphable):
     ``f_dtype`` torch.float16 / torch.bfloat16 stores fbar, the projector
     input, in 16 bits; the iterate f and all arithmetic stay FP32 (rounding f
     itself each iteration would drop updates below the 16-bit resolution).
+
+    ``exact`` (a plan of the same geometry with sampler "exact") corrects the
+    error of a texture-filtered ``plan`` ("pairs", "tex": 8-bit interpolation
+    weights, which a 100-iteration reconstruction amplifies to several 1e-3
+    of the FP64 result). Every ``correct_every`` iterations the exact plan
+    projects and backprojects the current iterate, and the differences
+    e_F = A_fast fbar - A_exact fbar and e_B = BP_exact w - BP_fast w are kept;
+    the iterations in between use A_fast fbar - e_F (as data g + e_F) and
+    BP_fast w + e_B. Their remaining error is the fast operators' error on
+    what fbar and w moved since the last refresh. Refresh iterations use the
+    exact operators themselves.
     """
 
     def __init__(self, plan: Plan, cascades: int = 30, sigma: float = 1e-7, tau: float = 1e-7,
                  mu: float = 1e5, v=(5e4, 5e4, 5e4), quirk: bool = True,
                  f_dtype=torch.float32, t_refresh: int = 10, use_graph: bool = False,
-                 backprojector: str = "fdk"):
+                 backprojector: str = "fdk", exact: Plan = None, correct_every: int = 10):
         if f_dtype not in _FDT:
             raise ValueError("f_dtype must be torch.float32, torch.float16 or torch.bfloat16")
         if backprojector not in ("fdk", "adjoint"):
             raise ValueError("backprojector must be 'fdk' or 'adjoint'")
+        if exact is not None:
+            if (tuple(exact.vol_shape(1)) != tuple(plan.vol_shape(1))
+                    or tuple(exact.sino_shape(1)) != tuple(plan.sino_shape(1))):
+                raise ValueError("the exact plan must have the geometry of the plan")
+            if int(correct_every) < 1:
+                raise ValueError("correct_every must be at least 1")
+        self.exact = exact
+        self.correct_every = int(correct_every)
         self.plan = plan
         self.cascades = int(cascades)
         self.sigma, self.tau, self.mu = float(sigma), float(tau), float(mu)
@@ -200,6 +219,11 @@ class DTVCP(_Graphable):
             "ws": torch.zeros(_lib.load().dtv_pdhg_workspace_bytes(), dtype=torch.uint8,
                               device=dev),
         }
+        if self.exact is not None:
+            for k in ("s1", "s2", "g_eff"):
+                st[k] = torch.empty(plan.sino_shape(b), dtype=torch.float32, device=dev)
+            for k in ("e_b", "t_vol"):
+                st[k] = torch.empty(vs, dtype=torch.float32, device=dev)
         return st
 
     def _body(self, st, image):
@@ -219,10 +243,31 @@ class DTVCP(_Graphable):
                 st["t"].zero_()
                 call("dtv_diff_abs_sums", _ptr(f), _lib.DTV_F32, size, b, prm.quirk,
                      _ptr(st["t"]), stream)
-            plan.forward(fbar, out=st["w"], epilogue=_lib.DTV_EPI_PDHG, g=st["g"],
-                         sigma=self.sigma, abs_sum=st["loss"][it:it + 1])
+            ex = self.exact
+            refresh = ex is not None and it % self.correct_every == 0
+            if refresh:
+                ns = st["w"].numel()
+                ex.forward(fbar, out=st["s1"])
+                plan.forward(fbar, out=st["s2"], epilogue=_lib.DTV_EPI_RESIDUAL, g=st["s1"])
+                call("dtv_lincomb", _ptr(st["g"]), 1.0, _ptr(st["s2"]), 1.0, _ptr(st["g_eff"]),
+                     ns, stream)  # data of the corrected projection: g + e_F
+                call("dtv_pdhg_sino_dual", _ptr(st["w"]), _ptr(st["s1"]), _ptr(st["g"]),
+                     self.sigma, ns, _ptr(st["loss"][it:it + 1]), stream)
+            else:
+                plan.forward(fbar, out=st["w"], epilogue=_lib.DTV_EPI_PDHG,
+                             g=st["g_eff"] if ex is not None else st["g"], sigma=self.sigma,
+                             abs_sum=st["loss"][it:it + 1])
             if self.backprojector == "fdk":
-                plan.backward(st["w"], out=st["recon"])
+                if ex is None:
+                    plan.backward(st["w"], out=st["recon"])
+                elif refresh:
+                    ex.backward(st["w"], out=st["recon"])
+                    plan.backward(st["w"], out=st["t_vol"])
+                    call("dtv_lincomb", _ptr(st["recon"]), 1.0, _ptr(st["t_vol"]), -1.0,
+                         _ptr(st["e_b"]), st["recon"].numel(), stream)
+                else:
+                    st["recon"].copy_(st["e_b"])
+                    plan.backward(st["w"], out=st["recon"], accumulate=True)
             else:
                 plan.adjoint(st["w"], out=st["recon"])
             call("dtv_pdhg_dual", _ptr(fbar), _ptr(st["p"]), _ptr(st["q"]), _ptr(st["s"]),

@@ -130,7 +130,7 @@ def check_input(t: torch.Tensor, name: str, shape=None, dtypes=(torch.float32,))
         raise RuntimeError(f"{name} must have shape {tuple(shape)}, got {tuple(t.shape)}")
 
 
-SAMPLERS = ("soft", "tex", "pairs", "tma")
+SAMPLERS = ("soft", "tex", "pairs", "tma", "exact")
 
 
 class Plan:
@@ -141,8 +141,12 @@ class Plan:
     bilinear fetch per sample, z interpolated in FP32) or "tma" (the same
     z-pairs streamed by the Tensor Memory Accelerator into shared memory per
     ray tile and interpolated there with FP32 weights; a tunable share of the
-    tiles still uses the texture unit). The backprojector samples the
-    sinogram through a texture for "tex", "pairs" and "tma".
+    tiles still uses the texture unit) or "exact" (the same FP16 z-pairs in a
+    zero-bordered linear copy read through L1, FP32 x/y/z weights, and the
+    software FP32-weight backprojector: no 8-bit texture weights anywhere,
+    whose error 100-iteration reconstructions amplify past 1e-3 of FP64).
+    The backprojector samples the sinogram through a texture for "tex",
+    "pairs" and "tma".
     ``stage_f16`` stages projected volumes as FP16 ("soft"/"tex").
     ``adjoint`` keeps a per-ray table (32 bytes per ray and view) and cell
     records (16 bytes per voxel) that speed up :meth:`adjoint`.
@@ -166,7 +170,8 @@ class Plan:
         self.sampler = sampler
         self.stage_f16 = bool(stage_f16)
         flags = {"soft": 0, "tex": _lib.DTV_PLAN_TEX, "pairs": _lib.DTV_PLAN_TEX_PAIRS,
-                 "tma": _lib.DTV_PLAN_TEX_PAIRS | _lib.DTV_PLAN_TMA}[sampler] | \
+                 "tma": _lib.DTV_PLAN_TEX_PAIRS | _lib.DTV_PLAN_TMA,
+                 "exact": _lib.DTV_PLAN_PAIRS_EXACT}[sampler] | \
             (_lib.DTV_PLAN_STAGE_F16 if stage_f16 else 0) | (_lib.DTV_PLAN_ADJOINT if adjoint else 0)
         h = ctypes.c_void_p()
         call("dtv_plan_create", ctypes.byref(geometry.struct), self.max_batch, flags,

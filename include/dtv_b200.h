@@ -84,6 +84,15 @@ extern "C" {
  * trilinear of the FP16 volume). DTV_TUNE_FP_TEX_SHARE sends a share of the
  * tiles through the texture unit instead, so both pipes work at once. */
 #define DTV_PLAN_TMA 0x10
+/* Exact interpolation weights in both directions. Forward projector: the FP16
+ * z pairs of DTV_PLAN_TEX_PAIRS staged in a linear array with a two-texel
+ * zero border, read through L1 (four 4-byte loads per sample) and
+ * interpolated with FP32 x/y/z weights (exact trilinear of the FP16-rounded
+ * volume). Backprojector: software bilinear with FP32 weights, as
+ * DTV_PLAN_SOFT. The texture filter's 8-bit weights, whose error iterative
+ * reconstructions amplify, are not used. Exclusive with DTV_PLAN_TEX,
+ * DTV_PLAN_TEX_PAIRS and DTV_PLAN_TMA. */
+#define DTV_PLAN_PAIRS_EXACT 0x20
 
 /* ---- forward-projector epilogues ---------------------------------------- */
 #define DTV_EPI_STORE 0    /* out = FP(vol)                                        */
@@ -399,6 +408,17 @@ DTV_API int dtv_tv_descent(const float* f_in, float* f_out, const int32_t size[3
  * data-dependent step sizes such as davg = alpha * dp on the GPU, ASDPOCS.py:35). */
 DTV_API int dtv_scale_scalar(const double* in, double scale, float* out, void* stream);
 
+/* out = a*x + b*y over n elements (out may alias x or y). No counterpart in the
+ * reference: the operator-error correction of DTVCP (exact minus fast
+ * projection, added to the fast one). */
+DTV_API int dtv_lincomb(const float* x, float a, const float* y, float b, float* out, int64_t n,
+                        void* stream);
+/* The PDHG sinogram dual step from a finished projection fp (DTVCP.py:38-39):
+ * w = (w + sigma*(fp - g))/(1 + sigma); abs_sum[0] += sum|fp - g| (device
+ * double, may be NULL). The forward projector's DTV_EPI_PDHG epilogue does the
+ * same inside the projection. */
+DTV_API int dtv_pdhg_sino_dual(float* w, const float* fp, const float* g, float sigma, int64_t n,
+                               double* abs_sum, void* stream);
 /* sum[0] += sum |a - b| over n elements (device double): ASD-POCS's
  * l1_loss(f, f0) as a sum (model/PDHG/ASDPOCS.py:44). */
 DTV_API int dtv_l1_distance(const float* a, const float* b, int64_t n, double* sum, void* stream);
@@ -418,6 +438,11 @@ DTV_API int dtv_asd_adapt(const double* dp_sum, const double* dg_sum, float rmax
  * texels: texel_bits 32 (half2, the forward projector's z-pair texel, and the
  * rate of the FP32 sinogram texels) or 64 (half4). */
 DTV_API int dtv_measure_texture_fetch_rate(int32_t texel_bits, double* fetches_per_second);
+/* The same fetch pattern on a 2-D array that holds the 64 planes as an 8 x 8
+ * grid of tiles (texture gather works on 2-D arrays only): gather 0, bilinear
+ * fetches of half2 texels; gather 1, gathers (the four unfiltered 32-bit
+ * texels of a bilinear footprint in one fetch). */
+DTV_API int dtv_measure_texture_gather_rate(int32_t gather, double* fetches_per_second);
 /* 16-byte float4 atomicAdd reductions per second into `records` records
  * ([1024, 2^26]; 72 MB = 4.7M records stays in L2): pattern 0, each warp's
  * 32 lanes on 32 consecutive records (the adjoint's neighbouring rays);
