@@ -955,7 +955,10 @@ def run_profile(args):
         plan.set_tuning(dtvb200._lib.DTV_TUNE_FP_BAND, args.fp_band)
     sino = poisson_noise(plan.forward(truth), c["i0"], seed=c["seed"])
     prm = dtv_params(plan, dev)
-    alg = dtvb200.DTVCP(plan, args.profile, t_refresh=10, use_graph=False, **prm)
+    K = args.correct_every if args.sampler in ("pairs", "tex", "tma") else 0
+    xplan = dtvb200.Plan(geo, max_batch=1, sampler="exact", device=dev) if K else None
+    alg = dtvb200.DTVCP(plan, args.profile, t_refresh=10, use_graph=False, exact=xplan,
+                        correct_every=max(K, 1), **prm)
     f = alg.run(torch.zeros(plan.vol_shape(1), device=dev), sino)
     torch.cuda.synchronize()
     print(json.dumps({"profile_iterations": args.profile, "sampler": args.sampler,
@@ -974,7 +977,7 @@ def main():
     ap.add_argument("--small", action="store_true", help="64^3 smoke-size workload")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--correct-every", type=int, default=10, metavar="K",
+    ap.add_argument("--correct-every", type=int, default=8, metavar="K",
                     help="refresh the exact-weight correction of a texture-filtered sampler "
                          "every K DTV iterations (0: uncorrected)")
     ap.add_argument("--no-check", action="store_true",

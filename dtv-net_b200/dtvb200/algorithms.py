@@ -149,13 +149,16 @@ class DTVCP(_Graphable):
     the iterations in between use A_fast fbar - e_F (as data g + e_F) and
     BP_fast w + e_B. Their remaining error is the fast operators' error on
     what fbar and w moved since the last refresh. Refresh iterations use the
-    exact operators themselves.
+    exact operators themselves. ``correct_bp_every`` sets the backprojector's
+    refresh interval apart (default: ``correct_every``); 1 backprojects with
+    the exact plan in every iteration.
     """
 
     def __init__(self, plan: Plan, cascades: int = 30, sigma: float = 1e-7, tau: float = 1e-7,
                  mu: float = 1e5, v=(5e4, 5e4, 5e4), quirk: bool = True,
                  f_dtype=torch.float32, t_refresh: int = 10, use_graph: bool = False,
-                 backprojector: str = "fdk", exact: Plan = None, correct_every: int = 10):
+                 backprojector: str = "fdk", exact: Plan = None, correct_every: int = 8,
+                 correct_bp_every: int = None):
         if f_dtype not in _FDT:
             raise ValueError("f_dtype must be torch.float32, torch.float16 or torch.bfloat16")
         if backprojector not in ("fdk", "adjoint"):
@@ -164,10 +167,12 @@ class DTVCP(_Graphable):
             if (tuple(exact.vol_shape(1)) != tuple(plan.vol_shape(1))
                     or tuple(exact.sino_shape(1)) != tuple(plan.sino_shape(1))):
                 raise ValueError("the exact plan must have the geometry of the plan")
-            if int(correct_every) < 1:
-                raise ValueError("correct_every must be at least 1")
+            if int(correct_every) < 1 or (correct_bp_every is not None and
+                                          int(correct_bp_every) < 1):
+                raise ValueError("correction intervals must be at least 1")
         self.exact = exact
         self.correct_every = int(correct_every)
+        self.correct_bp_every = int(correct_bp_every) if correct_bp_every else int(correct_every)
         self.plan = plan
         self.cascades = int(cascades)
         self.sigma, self.tau, self.mu = float(sigma), float(tau), float(mu)
@@ -257,10 +262,13 @@ class DTVCP(_Graphable):
                 plan.forward(fbar, out=st["w"], epilogue=_lib.DTV_EPI_PDHG,
                              g=st["g_eff"] if ex is not None else st["g"], sigma=self.sigma,
                              abs_sum=st["loss"][it:it + 1])
+            bp_refresh = ex is not None and it % self.correct_bp_every == 0
             if self.backprojector == "fdk":
                 if ex is None:
                     plan.backward(st["w"], out=st["recon"])
-                elif refresh:
+                elif self.correct_bp_every == 1:
+                    ex.backward(st["w"], out=st["recon"])
+                elif bp_refresh:
                     ex.backward(st["w"], out=st["recon"])
                     plan.backward(st["w"], out=st["t_vol"])
                     call("dtv_lincomb", _ptr(st["recon"]), 1.0, _ptr(st["t_vol"]), -1.0,
