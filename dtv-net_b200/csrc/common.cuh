@@ -65,12 +65,11 @@ __device__ __forceinline__ __half2 u32_as_half2(unsigned int w) {
                         __ushort_as_half((unsigned short)(w >> 16)));
 }
 
-// Record of padded column (X, Y) = (x + 2, y + 2) and z-pair layer L in the
-// 2 x 2 x 2-brick order of the exact sampler's records.
-__device__ __forceinline__ int pair_quad_index(int X, int Y, int L, int bx, int by) {
-  return ((((L >> 1) * by + (Y >> 1)) * bx + (X >> 1)) << 3) | ((L & 1) << 2) | ((Y & 1) << 1) |
-         (X & 1);
-}
+// Zero border of the exact sampler's records (texels on each side in x and y,
+// layers in z). The ray set-up keeps every sample within one step of (-1, n)
+// on each axis, so its cell corner lies in [-2, n] and a border of 3 leaves a
+// whole texel of slack for the FP32 rounding of the sample positions.
+constexpr int kQuadPad = 3;
 
 inline int dtype_size(int dt) { return dt == DTV_F32 ? 4 : 2; }
 inline bool dtype_ok(int dt) { return dt == DTV_F32 || dt == DTV_F16 || dt == DTV_BF16; }
@@ -156,12 +155,11 @@ struct Plan {
   unsigned int* d_pair_lin;
   int pair_pitch;
   // exact z-pair sampler (DTV_PLAN_PAIRS_EXACT): per batch item, 16-byte
-  // records (x, y, L) of the four x/y corner words of a z-pair cell over the
-  // grid padded by two zero texels in x and y, in 2 x 2 x 2 bricks of
-  // 128 bytes (pair_quad_index)
+  // records [L][Y][X] of the four x/y corner words of a z-pair cell, over the
+  // grid padded by kQuadPad zero texels on every side (X = x + 3, Y = y + 3,
+  // L = floor(z) + 3 holds (f[L-3], f[L-2]))
   uint4* d_pair_quad;
   int64_t pair_quad_elems;  // records per batch item
-  int quad_bx, quad_by;     // bricks along x and y
   int fp_tex_share;          // DTV_TUNE_FP_TEX_SHARE
   alignas(64) unsigned char tmap[2][128];
   int* d_status;             // device error bits

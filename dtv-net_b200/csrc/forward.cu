@@ -69,32 +69,51 @@ struct QuadSampler {
   }
 };
 
+// Packed FP32 pairs (Blackwell's two-lane FP32 arithmetic): the z-pair
+// samplers interpolate both planes of a cell in one instruction.
+__device__ __forceinline__ unsigned long long f32x2(float lo, float hi) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ unsigned long long f32x2_lerp(unsigned long long w,
+                                                         unsigned long long a,
+                                                         unsigned long long b) {
+  unsigned long long d, r;  // a + w (b - a), each lane rounded as fmaf(w, b - a, a)
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(b), "l"(a));
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(w), "l"(d), "l"(a));
+  return r;
+}
+__device__ __forceinline__ unsigned long long half2_to_f32x2(unsigned int w) {
+  const float2 f = __half22float2(u32_as_half2(w));
+  return f32x2(f.x, f.y);
+}
+
 // Exact trilinear sample of the FP16 z pairs (DTV_PLAN_PAIRS_EXACT): one
-// 16-byte record holds the four x/y corner words of the sample's cell, word =
-// (f[L-2], f[L-1]) at layer L = floor(z) + 2, so a sample is one 128-bit load
-// through L1 and FP32 x/y/z weights. Positions arrive in voxel index
-// coordinates; the ray set-up keeps them within one step of (-1, n), and the
-// clamps keep every record inside the zero-padded grid whatever the rounding.
+// 16-byte record [L][Y][X] holds the four x/y corner words of the sample's
+// cell, word = (f[fz], f[fz+1]) at layer L = floor(z) + 3, so a sample is one
+// 128-bit load through L1 and FP32 x/y/z weights (x, then y, then z, as
+// SoftSampler; both planes at once in packed FP32). Positions arrive in voxel
+// index coordinates within one step of (-1, n) (the ray set-up), inside the
+// kQuadPad border; the record index is clamped into the array all the same,
+// so no position can address memory outside it.
 struct PairQuadSampler {
-  const uint4* rec;    // records of this batch item
-  int bx, by;          // bricks along x and y
-  float mx, my, lmax;  // nx, ny, nz + 2
+  const uint4* rec;  // records of this batch item, shifted to (x, y, z) = (0, 0, 0)
+  float px;          // records per row (nx + 6)
+  int plane;         // records per layer
+  int lo, hi;        // valid record offsets from rec: [lo, hi]
   __device__ __forceinline__ float operator()(float x, float y, float z) const {
     const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
     const float ax = x - fx, ay = y - fy, az = z - fz;
-    const int X = (int)fminf(fmaxf(fx, -2.f), mx) + 2;
-    const int Y = (int)fminf(fmaxf(fy, -2.f), my) + 2;
-    const int L = (int)fminf(fmaxf(fz + 2.f, 0.f), lmax);
-    const uint4 r = __ldg(rec + pair_quad_index(X, Y, L, bx, by));
-    const float2 c00 = __half22float2(u32_as_half2(r.x));
-    const float2 c10 = __half22float2(u32_as_half2(r.y));
-    const float2 c01 = __half22float2(u32_as_half2(r.z));
-    const float2 c11 = __half22float2(u32_as_half2(r.w));
-    // lerps in the order of SoftSampler: x, then y, then z
-    const float a0 = fmaf(ax, c10.x - c00.x, c00.x), a1 = fmaf(ax, c11.x - c01.x, c01.x);
-    const float b0 = fmaf(ax, c10.y - c00.y, c00.y), b1 = fmaf(ax, c11.y - c01.y, c01.y);
-    const float lo = fmaf(ay, a1 - a0, a0), hi = fmaf(ay, b1 - b0, b0);
-    return fmaf(az, hi - lo, lo);
+    int q = (int)fz * plane + (int)fmaf(fy, px, fx);
+    q = min(max(q, lo), hi);
+    const uint4 r = __ldg(rec + q);
+    const unsigned long long wx = f32x2(ax, ax), wy = f32x2(ay, ay);
+    const unsigned long long a0 = f32x2_lerp(wx, half2_to_f32x2(r.x), half2_to_f32x2(r.y));
+    const unsigned long long a1 = f32x2_lerp(wx, half2_to_f32x2(r.z), half2_to_f32x2(r.w));
+    float lo0, hi0;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo0), "=f"(hi0) : "l"(f32x2_lerp(wy, a0, a1)));
+    return fmaf(az, hi0 - lo0, lo0);
   }
 };
 
@@ -221,8 +240,7 @@ __global__ void __launch_bounds__(kFPThreads) fp_pair_kernel(RayParams rp, const
 __global__ void __launch_bounds__(kFPThreads) fp_pairx_kernel(RayParams rp,
                                                               const FPView* __restrict__ views,
                                                               const uint4* __restrict__ rec,
-                                                              int64_t rec_elems, int bx, int by,
-                                                              FPOut o) {
+                                                              int64_t rec_elems, FPOut o) {
   int u, v, n;
   tile_pixel(rp, u, v, n);
   const int b = blockIdx.z;
@@ -230,12 +248,13 @@ __global__ void __launch_bounds__(kFPThreads) fp_pairx_kernel(RayParams rp,
   if (u < rp.nu && v < rp.nv) {
     const RaySetup rs = setup_ray(rp, views[n], u, v);
     PairQuadSampler smp;
-    smp.rec = rec + b * rec_elems;
-    smp.bx = bx;
-    smp.by = by;
-    smp.mx = (float)rp.nx;
-    smp.my = (float)rp.ny;
-    smp.lmax = (float)(rp.nz + 2);
+    const int px = rp.nx + 2 * kQuadPad;
+    smp.px = (float)px;
+    smp.plane = px * (rp.ny + 2 * kQuadPad);
+    const int origin = kQuadPad * smp.plane + kQuadPad * px + kQuadPad;
+    smp.rec = rec + b * rec_elems + origin;
+    smp.lo = -origin;
+    smp.hi = (int)rec_elems - 1 - origin;
     const float val = rs.count > 0 ? ray_sum(smp, rs) * rp.scale : 0.f;
     fp_store(rp, o, n, b, u, v, val, res);
   }
@@ -244,14 +263,14 @@ __global__ void __launch_bounds__(kFPThreads) fp_pairx_kernel(RayParams rp,
 
 // Writes the exact sampler's records of one volume: record (X, Y, L) =
 // words (X, Y), (X+1, Y), (X, Y+1), (X+1, Y+1) of z-pair layer L, word =
-// half2(f[L-2], f[L-1]) at padded column (X, Y) = (x + 2, y + 2), zero outside
-// the volume. Only records that reach the volume are written (X in [1, nx+1],
-// Y in [1, ny+1], L in [1, nz+1]); the others keep the plan's initial zeros.
+// half2(f[L-3], f[L-2]) at padded column (X, Y) = (x + 3, y + 3), zero outside
+// the volume. Only records that reach the volume are written (X in [2, nx+2],
+// Y in [2, ny+2], L in [2, nz+2]); the others keep the plan's initial zeros.
 // A thread owns one record column and kStageLayers layers of it.
 template <class Tin>
 __global__ void __launch_bounds__(256) stage_pair_quads_kernel(const Tin* __restrict__ in,
                                                                uint4* __restrict__ rec, int nx,
-                                                               int ny, int nz, int bx, int by);
+                                                               int ny, int nz);
 
 // Writes the z-pair layers of one volume: layer L = (f[L-2], f[L-1]), zero
 // outside [0, nz), to the layered texture and, when `lin` is set, to the
@@ -291,14 +310,14 @@ __global__ void __launch_bounds__(256) stage_pairs_kernel(const Tin* __restrict_
 template <class Tin>
 __global__ void __launch_bounds__(256) stage_pair_quads_kernel(const Tin* __restrict__ in,
                                                                uint4* __restrict__ rec, int nx,
-                                                               int ny, int nz, int bx, int by) {
-  const int X = blockIdx.x * 32 + (threadIdx.x & 31) + 1;
-  const int Y = blockIdx.y * 8 + (threadIdx.x >> 5) + 1;
-  if (X > nx + 1 || Y > ny + 1) return;
-  const int L0 = 1 + blockIdx.z * kStageLayers;
-  const int L1 = min(L0 + kStageLayers, nz + 2);
+                                                               int ny, int nz) {
+  const int X = blockIdx.x * 32 + (threadIdx.x & 31) + kQuadPad - 1;
+  const int Y = blockIdx.y * 8 + (threadIdx.x >> 5) + kQuadPad - 1;
+  if (X > nx + kQuadPad - 1 || Y > ny + kQuadPad - 1) return;
+  const int L0 = kQuadPad - 1 + blockIdx.z * kStageLayers;
+  const int L1 = min(L0 + kStageLayers, nz + kQuadPad);
   const int64_t plane = (int64_t)nx * ny;
-  const int x = X - 2, y = Y - 2;
+  const int x = X - kQuadPad, y = Y - kQuadPad;
   // the four columns of the record: (x, y), (x+1, y), (x, y+1), (x+1, y+1)
   const bool in_c[4] = {x >= 0 && y >= 0, x + 1 < nx && y >= 0, x >= 0 && y + 1 < ny,
                         x + 1 < nx && y + 1 < ny};
@@ -308,18 +327,21 @@ __global__ void __launch_bounds__(256) stage_pair_quads_kernel(const Tin* __rest
     return (in_c[c] && z >= 0 && z < nz) ? __float2half_rn(load_as_float(in + off[c], z * plane))
                                          : __float2half_rn(0.f);
   };
+  const int px = nx + 2 * kQuadPad;
+  const int64_t rplane = (int64_t)px * (ny + 2 * kQuadPad);
+  uint4* col = rec + (int64_t)Y * px + X;
   __half prev[4];
 #pragma unroll
-  for (int c = 0; c < 4; ++c) prev[c] = member(c, L0 - 2);
+  for (int c = 0; c < 4; ++c) prev[c] = member(c, L0 - kQuadPad);
   for (int L = L0; L < L1; ++L) {
     unsigned int wd[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      const __half cur = member(c, L - 1);
+      const __half cur = member(c, L - kQuadPad + 1);
       wd[c] = (unsigned int)__half_as_ushort(prev[c]) | ((unsigned int)__half_as_ushort(cur) << 16);
       prev[c] = cur;
     }
-    rec[pair_quad_index(X, Y, L, bx, by)] = make_uint4(wd[0], wd[1], wd[2], wd[3]);
+    col[L * rplane] = make_uint4(wd[0], wd[1], wd[2], wd[3]);
   }
 }
 
@@ -439,8 +461,7 @@ static int stage_volume_pairs(Plan* p, const Tin* vol, int batch, cudaStream_t s
       dim3 qg((g.nx + 1 + 31) / 32, (g.ny + 1 + 7) / 8, (g.nz + 1 + kStageLayers - 1) / kStageLayers);
       stage_pair_quads_kernel<Tin><<<qg, 256, 0, st>>>(vol + b * vox,
                                                        p->d_pair_quad + b * p->pair_quad_elems,
-                                                       g.nx, g.ny, g.nz, p->quad_bx,
-                                                       p->quad_by); note_launch();
+                                                       g.nx, g.ny, g.nz); note_launch();
     } else {
       unsigned int* lin =
           p->d_pair_lin ? p->d_pair_lin + (int64_t)b * p->pair_pitch * g.ny * (g.nz + 3) : nullptr;
@@ -489,7 +510,7 @@ int forward_impl(Plan* p, const void* vol, int vol_dtype, int batch, float* out,
     return fp_tma_launch(p, rp, o, batch, st);
   } else if (p->d_pair_quad) {
     fp_pairx_kernel<<<grid, kFPThreads, 0, st>>>(rp, p->d_fpv, p->d_pair_quad, p->pair_quad_elems,
-                                                 p->quad_bx, p->quad_by, o); note_launch();
+                                                 o); note_launch();
   } else if (pairs) {
     fp_pair_kernel<<<grid, kFPThreads, 0, st>>>(rp, p->d_fpv, p->pair_tex_dev, o); note_launch();
   } else if (tex) {

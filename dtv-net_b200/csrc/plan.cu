@@ -153,10 +153,8 @@ int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Pla
   // Staged volumes of the software sampler (FP32: quad records, FP16: the
   // padded volume): zero border written once here, interiors by each call.
   if (flags & DTV_PLAN_PAIRS_EXACT) {
-    p->quad_bx = (gp.nx + 4 + 1) / 2;
-    p->quad_by = (gp.ny + 4 + 1) / 2;
-    const int64_t bl = (gp.nz + 3 + 1) / 2;
-    p->pair_quad_elems = (int64_t)p->quad_bx * p->quad_by * bl * 8;
+    p->pair_quad_elems = (int64_t)(gp.nx + 2 * kQuadPad) * (gp.ny + 2 * kQuadPad) *
+                         (gp.nz + 2 * kQuadPad - 1);
     if (p->pair_quad_elems >= (1LL << 31)) {
       free_plan(p);
       return fail(DTV_ERR_UNSUPPORTED, "volume too large for DTV_PLAN_PAIRS_EXACT");

@@ -152,11 +152,12 @@ template <class Sampler>
 __device__ __forceinline__ float ray_sum(const Sampler& smp, const RaySetup& rs) {
   float a0 = 0.f, a1 = 0.f;
   int k = 0;
-  for (; k + 3 < rs.count; k += 4) {
+  float kb = 0.f;  // (float)k, advanced by exact integer additions
+  for (; k + 3 < rs.count; k += 4, kb += 4.f) {
     float s[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const float kf = (float)(k + j);
+      const float kf = kb + (float)j;
       s[j] = smp(fmaf(kf, rs.dp[0], rs.p0[0]), fmaf(kf, rs.dp[1], rs.p0[1]),
                  fmaf(kf, rs.dp[2], rs.p0[2]));
     }
