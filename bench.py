@@ -871,6 +871,58 @@ def fista64_cpu(c, truth_np, sigma, v):
             "sample": "the whole step (FP + BP + 20 FISTA-DTV iterations), FP64 oracle, once"}
 
 
+def fp64_check_large(dev, sampler, K, iters):
+    """Checker leg of the large workload, outside its timed region, on its
+    stated downsample: 128^3 x 4 mm with a 256x192 detector at 3.2 mm (the
+    field of view of 512^3 x 1 mm, 1024x768 @ 0.8 mm) and 64 views. Relative
+    RMSE vs the FP64 oracle of the forward projection (FP32- and BF16-stored
+    volume), the FDK backprojection, and the `iters`-iteration DTV
+    reconstruction with FP32 and BF16 fbar, corrected every K iterations as
+    the timed run."""
+    import numpy as np
+    import torch
+
+    import dtvb200
+    from dtvb200.phantom import ellipsoids
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as O
+
+    def rel(a, b):
+        a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+        return float(np.sqrt(np.mean((a - b) ** 2) / np.mean(b ** 2)))
+
+    t0 = time.perf_counter()
+    ang = np.linspace(0, 360, 64, endpoint=False)
+    args = (ang, (128, 128, 128), (4.0,) * 3, (256, 192), (3.2, 3.2), 500.0, 1000.0)
+    geo, og = dtvb200.circular(*args), O.circular_geometry(*args)
+    truth = ellipsoids((128, 128, 128), seed=CFG["seed"], device=dev)
+    plan = dtvb200.Plan(geo, max_batch=1, sampler=sampler, device=dev)
+    xplan = dtvb200.Plan(geo, max_batch=1, sampler="exact", device=dev) if K else None
+    tn = truth.cpu().numpy()
+    ref = O.forward(og, tn).reshape(1, 1, *og.sino_shape)
+    out = {"forward_fp32_volume": rel(plan.forward(truth).cpu().numpy(), ref),
+           "forward_bf16_volume": rel(plan.forward(truth.to(torch.bfloat16)).cpu().numpy(), ref)}
+    sino = torch.from_numpy(ref.astype(np.float32)).to(dev)
+    out["backward"] = rel(plan.backward(sino).cpu().numpy(),
+                          O.backward(og, ref).reshape(1, 1, *og.vol_shape))
+    prm = dtv_params(plan, dev)
+    fpo = lambda x: O.forward(og, x).reshape(x.shape[0], 1, *og.sino_shape)  # noqa: E731
+    bpo = lambda s: O.backward(og, s).reshape(s.shape[0], 1, *og.vol_shape)  # noqa: E731
+    rec = O.dtvcp_run(fpo, bpo, np.zeros((1, 1) + og.vol_shape), ref, (128, 128, 128), iters,
+                      prm["sigma"], prm["tau"], prm["mu"], prm["v"], quirk=prm["quirk"])
+    for name, dt in (("reconstruction_fp32_fbar", torch.float32),
+                     ("reconstruction_bf16_fbar", torch.bfloat16)):
+        alg = dtvb200.DTVCP(plan, iters, t_refresh=10, use_graph=True, f_dtype=dt, exact=xplan,
+                            correct_every=max(K, 1), **prm)
+        out[name] = rel(alg.run(torch.zeros(plan.vol_shape(1), device=dev), sino).cpu().numpy(),
+                        rec)
+    out.update(gate=1e-3, seconds=time.perf_counter() - t0,
+               how=(f"relative RMSE vs the FP64 oracle on the stated downsample: 128^3 x 4 mm, "
+                    f"256x192 det @ 3.2 mm, 64 views over 360 deg; {iters} DTV-PDHG iterations "
+                    f"from the noiseless projection of the same phantom"))
+    return out
+
+
 def run_large512(args):
     """Large: 512^3 ellipsoid phantom (1 mm voxels), 1024x768 detector at
     0.8 mm pitch, SOD 500 / SDD 1000. One step = the 360-view full-scan forward
@@ -892,6 +944,9 @@ def run_large512(args):
     full = dtvb200.Plan(geo, max_batch=1, sampler=args.sampler, device=dev)
     plan = dtvb200.Plan(geo_s, max_batch=1, sampler=args.sampler, device=dev)
     prm = dtv_params(plan, dev, iters=4)
+    K = args.correct_every if args.sampler in ("pairs", "tex", "tma") else 0
+    corr = dict(exact=dtvb200.Plan(geo_s, max_batch=1, sampler="exact", device=dev) if K else None,
+                correct_every=max(K, 1))
     sino_full = torch.empty(full.sino_shape(1), device=dev)
     V = n ** 3
     units = full.fp_samples() + iters * (plan.fp_samples() + V * sparse)
@@ -899,7 +954,7 @@ def run_large512(args):
     res = {}
     for name, dt in (("fp32", torch.float32), ("bf16", torch.bfloat16)):
         vol = truth.to(dt)
-        alg = dtvb200.DTVCP(plan, iters, t_refresh=10, use_graph=True, f_dtype=dt, **prm)
+        alg = dtvb200.DTVCP(plan, iters, t_refresh=10, use_graph=True, f_dtype=dt, **corr, **prm)
         img = torch.zeros(plan.vol_shape(1), device=dev)
 
         def step():
@@ -913,7 +968,10 @@ def run_large512(args):
                      "launches": alg.launches_per_run + 2}
     err = float(torch.sqrt(((res["bf16"]["f"] - res["fp32"]["f"]).double() ** 2).mean()
                            / (res["fp32"]["f"].double() ** 2).mean()))
-    secs = res["fp32"]["secs"]
+    secs, bf16_secs = res["fp32"]["secs"], res["bf16"]["secs"]
+    launches, clocks = res["fp32"]["launches"], res["fp32"]["clocks"]
+    del res, full, plan, corr, sino_full
+    check = None if args.no_check else fp64_check_large(dev, args.sampler, K, iters)
     line = {
         "metric": METRIC, "value": units * args.steps / secs / 1e9, "unit": UNIT, "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
@@ -921,15 +979,41 @@ def run_large512(args):
         "data": "synthetic",
         "config": {"workload": "512^3 x 1 mm, 1024x768 det @ 0.8 mm, SOD 500 SDD 1000: 360-view "
                                "full-scan FP + 50 DTV iterations on the 90-view subset",
-                   "sampler": args.sampler, "graph": "one CUDA graph per reconstruction"},
+                   "sampler": args.sampler, "graph": "one CUDA graph per reconstruction",
+                   "correction": (f"operators corrected by the exact-weight plan every {K} "
+                                  f"iterations" if K else None)},
         "recon_per_s": args.steps / secs,
-        "bf16_storage": {"value": units * args.steps / res["bf16"]["secs"] / 1e9,
-                         "recon_per_s": args.steps / res["bf16"]["secs"],
+        "bf16_storage": {"value": units * args.steps / bf16_secs / 1e9,
+                         "recon_per_s": args.steps / bf16_secs,
                          "rel_rmse_vs_fp32_storage": err},
-        "gpu_launches": res["fp32"]["launches"] * args.steps,
-        "clocks": res["fp32"]["clocks"],
+        "error_vs_fp64": check,
+        "gpu_launches": launches * args.steps,
+        "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_peaks(args):
+    """The roofline denominators of the projectors and the adjoint, measured on
+    this GPU (each rate three times): bilinear texture fetches of 32- and
+    64-bit texels from a layered texture, bilinear fetches and gathers from a
+    tiled 2-D texture, and 16-byte L2 vector reductions."""
+    import torch
+
+    import dtvb200
+    L = dtvb200._lib
+    torch.cuda.init()
+    rates = {
+        "bilinear_layered_32bit": [L.measure_texture_fetch_rate(32) for _ in range(3)],
+        "bilinear_layered_64bit": [L.measure_texture_fetch_rate(64) for _ in range(3)],
+        "bilinear_tiled2d_32bit": [L.measure_texture_gather_rate(0) for _ in range(3)],
+        "gather_tiled2d_32bit": [L.measure_texture_gather_rate(1) for _ in range(3)],
+        "atomic_v4_contiguous": [L.measure_atomic_v4_rate(72 << 16, 0) for _ in range(3)],
+        "atomic_v4_scattered": [L.measure_atomic_v4_rate(72 << 16, 1) for _ in range(3)],
+    }
+    print(json.dumps({"unit": "per second", "sm_count": torch.cuda.get_device_properties(
+        0).multi_processor_count, "rates": rates}), flush=True)
     return 0
 
 
@@ -983,7 +1067,7 @@ def main():
     ap.add_argument("--no-check", action="store_true",
                     help="skip the FP64 error check and the reference-CUDA baseline")
     ap.add_argument("--workload", choices=["sparse_dtv", "batch16", "train", "fista64",
-                                           "large512"],
+                                           "large512", "peaks"],
                     default="sparse_dtv",
                     help="sparse_dtv: the headline workload; batch16: 16 heterogeneous FISTA "
                          "reconstructions batched into one graph; train: training steps of a "
@@ -1011,6 +1095,8 @@ def main():
         return run_fista64(args)
     if args.workload == "large512":
         return run_large512(args)
+    if args.workload == "peaks":
+        return run_peaks(args)
     return run_ours(args)
 
 
