@@ -191,7 +191,7 @@ def op_profile(plan, alg, img, sino, dev):
     import dtvb200
     from dtvb200 import _lib
     from dtvb200.geometry import _ptr, _stream
-    key = (tuple(img.shape), img.device.index)
+    key = (tuple(img.shape), img.device.index, alg._fused())
     st = alg._state[key]
     prm = alg._params()
     size = _lib.ivec(plan.geometry.volume_size)
@@ -500,7 +500,16 @@ def run_ours(args):
     # ---- per-operator profile (eager pass with events on the launching stream)
     t_fp, t_bp, t_up = op_profile(plan, alg, img, sino, dev)
     t_xfp = t_xbp = 0.0
-    if xplan is not None:  # the exact operators of each correction, timed alone
+    if xplan is not None and alg._fused():  # the one-launch correction passes, timed alone
+        vol = img + 0.5
+        w_, ge_ = torch.zeros_like(sino), torch.empty_like(sino)
+        xv, eb_ = torch.empty(plan.vol_shape(1), device=dev), torch.empty(plan.vol_shape(1),
+                                                                            device=dev)
+        t_xfp = time_steps(lambda: dtvb200.forward_refresh(plan, xplan, vol, sino, w_, ge_, 0.1),
+                           5, stream) / 5 * 1e3
+        t_xbp = time_steps(lambda: dtvb200.backward_refresh(plan, xplan, sino, xv, eb_), 5,
+                           stream) / 5 * 1e3
+    elif xplan is not None:  # the exact operators of each correction, timed alone
         xs = torch.empty(plan.sino_shape(1), device=dev)
         xv = torch.empty(plan.vol_shape(1), device=dev)
         t_xfp = time_steps(lambda: xplan.forward(img + 0.5, out=xs), 5, stream) / 5 * 1e3
@@ -575,7 +584,10 @@ def run_ours(args):
         "samples_per_recon": units,
         "per_iteration_ms": {"total": secs / args.steps / c["iters"] * 1e3, "forward": t_fp,
                              "backward": t_bp, "updates": t_up,
-                             "exact_forward": t_xfp or None, "exact_backward": t_xbp or None,
+                             ("refresh_forward" if alg._fused() else "exact_forward"):
+                                 t_xfp or None,
+                             ("refresh_backward" if alg._fused() else "exact_backward"):
+                                 t_xbp or None,
                              "correct_every": K or None},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak,

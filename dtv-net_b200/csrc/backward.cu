@@ -74,8 +74,20 @@ struct QuadBil {
   }
 };
 
-// Where the backprojector's detector values come from.
-enum BPSource { kSrcSoft = 0, kSrcTex = 1, kSrcQuad = 2 };
+// Where the backprojector's detector values come from. kSrcBoth: the texture
+// and the quad records of the same sinogram, two sums per voxel (the
+// correction pass of a texture-filtered plan against an exact one).
+enum BPSource { kSrcSoft = 0, kSrcTex = 1, kSrcQuad = 2, kSrcBoth = 3 };
+
+// Where a block's sums go: out = base + sum (out = sum when base is NULL; base
+// may be out). kSrcBoth: out takes the quad-record sum E, and
+// diff = diff_base + (E - T) with T the texture sum.
+struct BPOut {
+  float* out;
+  const float* base;
+  float* diff;
+  const float* diff_base;
+};
 
 // kZAff: every view's u and h are independent of z (a detector parallel to the
 // rotation axis, as in the circular orbits), so per column and view the kernel
@@ -97,8 +109,7 @@ struct TableMaps {
 template <int kSrc, bool kZAff, int ZC, class Maps>
 __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps, int n0, int n_chunk,
                                            const float* __restrict__ spad, cudaTextureObject_t tex,
-                                           float* __restrict__ out, int accumulate, int tile,
-                                           int zc) {
+                                           const BPOut& dst, int tile, int zc) {
   const int tiles_x = (bp.nx + kBPTile - 1) / kBPTile;
   // this thread's column in the 16 x 16 tile; a warp covers 16 x 2, 8 x 4 or
   // 4 x 8 columns (the narrower, the fewer detector rows' cache sectors one
@@ -130,9 +141,12 @@ __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps,
   const int j = (tile / tiles_x) * kBPTile + lj;
   const int k0 = zc * ZC;
   if (i >= bp.nx || j >= bp.ny) return;
-  float acc[ZC];
+  constexpr bool kBoth = kSrc == kSrcBoth;
+  float acc[ZC], act[kBoth ? ZC : 1];
 #pragma unroll
   for (int z = 0; z < ZC; ++z) acc[z] = 0.f;
+#pragma unroll
+  for (int z = 0; z < (kBoth ? ZC : 1); ++z) act[z] = 0.f;
   const float fi = (float)i, fj = (float)j;
   const int pu = bp.nu + 2 * kPad;
   const float mu = (float)bp.nu, mv = (float)bp.nv;
@@ -145,31 +159,36 @@ __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps,
     const float bu = fmaf(m0, fi, fmaf(m1, fj, m3));
     const float bv = fmaf(m4, fi, fmaf(m5, fj, m7));
     const float bh = fmaf(m8, fi, fmaf(m9, fj, m11));
-    using Smp = typename std::conditional<kSrc == kSrcQuad, QuadBil, SoftBil>::type;
+    using Smp = typename std::conditional<kSrc == kSrcQuad || kBoth, QuadBil, SoftBil>::type;
     Smp smp;
-    if constexpr (kSrc == kSrcQuad)
+    if constexpr (kSrc == kSrcQuad || kBoth)
       smp = QuadBil{reinterpret_cast<const float4*>(spad) + (int64_t)n * bp.sino_pad_elems, pu,
                     mu, mv};
     else
       smp = SoftBil{spad + (int64_t)n * bp.sino_pad_elems, pu, mu, mv};
     if constexpr (kZAff) {
       const float rh = __frcp_rn(bh);
-      // v from the absolute slice index: the same bits for every z-chunking
-      const float u = bu * rh, vb = bv * rh, dv = m6 * rh;
+      // v from the absolute slice index: the same bits for every z-chunking.
+      // Coordinates are rounded explicitly (no contraction into FMAs), so
+      // every kernel instance samples a voxel-view at the same position.
+      const float u = __fmul_rn(bu, rh), vb = __fmul_rn(bv, rh), dv = __fmul_rn(m6, rh);
+      const float tu = __fadd_rn(u, 0.5f);  // texture coordinate (texel centres at i + 1/2)
       float wgt = bp.scale;
       if (bp.power == 2) wgt *= rh * rh;
       else if (bp.power == 1) wgt *= rh;
-      const bool col_out = bp.extent && (u + 0.5f < -1.f || u + 0.5f > bp.nx + 1.f);
+      const bool col_out = bp.extent && (tu < -1.f || tu > bp.nx + 1.f);
       if (col_out) continue;
 #pragma unroll
       for (int z = 0; z < ZC; ++z) {
         const float v = fmaf((float)(k0 + z), dv, vb);
+        const float tv = __fadd_rn(v, 0.5f);
         float wz = wgt;
-        if (bp.extent && (v + 0.5f < -1.f || v + 0.5f > bp.ny + 1.f)) wz = 0.f;
+        if (bp.extent && (tv < -1.f || tv > bp.ny + 1.f)) wz = 0.f;
         float val;
-        if constexpr (kSrc == kSrcTex) val = tex2DLayered<float>(tex, u + 0.5f, v + 0.5f, n);
+        if constexpr (kSrc == kSrcTex) val = tex2DLayered<float>(tex, tu, tv, n);
         else val = smp(u, v);
         acc[z] = fmaf(val, wz, acc[z]);
+        if constexpr (kBoth) act[z] = fmaf(tex2DLayered<float>(tex, tu, tv, n), wz, act[z]);
       }
     } else {
 #pragma unroll
@@ -177,30 +196,34 @@ __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps,
         const float fk = (float)(k0 + z);
         const float h = fmaf(m10, fk, bh);
         const float rh = __frcp_rn(h);
-        const float u = fmaf(m2, fk, bu) * rh;
-        const float v = fmaf(m6, fk, bv) * rh;
+        const float u = __fmul_rn(fmaf(m2, fk, bu), rh);
+        const float v = __fmul_rn(fmaf(m6, fk, bv), rh);
+        const float tu = __fadd_rn(u, 0.5f), tv = __fadd_rn(v, 0.5f);
         float wgt = bp.scale;
         if (bp.power == 2) wgt *= rh * rh;
         else if (bp.power == 1) wgt *= rh;
-        if (bp.extent) {
-          const float tx = u + 0.5f, ty = v + 0.5f;
-          if (tx < -1.f || tx > bp.nx + 1.f || ty < -1.f || ty > bp.ny + 1.f) wgt = 0.f;
-        }
+        if (bp.extent && (tu < -1.f || tu > bp.nx + 1.f || tv < -1.f || tv > bp.ny + 1.f))
+          wgt = 0.f;
         float val;
-        if constexpr (kSrc == kSrcTex) val = tex2DLayered<float>(tex, u + 0.5f, v + 0.5f, n);
+        if constexpr (kSrc == kSrcTex) val = tex2DLayered<float>(tex, tu, tv, n);
         else val = smp(u, v);
         acc[z] = fmaf(val, wgt, acc[z]);
+        if constexpr (kBoth) act[z] = fmaf(tex2DLayered<float>(tex, tu, tv, n), wgt, act[z]);
       }
     }
   }
   const int64_t plane = (int64_t)bp.nx * bp.ny;
-  float* o = out + (int64_t)j * bp.nx + i;
+  const int64_t col = (int64_t)j * bp.nx + i;
 #pragma unroll
   for (int z = 0; z < ZC; ++z) {
     const int k = k0 + z;
     if (k < bp.nz) {
-      if (accumulate) o[k * plane] += acc[z];
-      else o[k * plane] = acc[z];
+      const int64_t e = col + k * plane;
+      dst.out[e] = dst.base ? dst.base[e] + acc[z] : acc[z];
+      if constexpr (kBoth) {
+        const float d = acc[z] - act[z];
+        dst.diff[e] = dst.diff_base ? dst.diff_base[e] + d : d;
+      }
     }
   }
 }
@@ -209,9 +232,8 @@ template <int kSrc, bool kZAff, int ZC>
 __global__ void __launch_bounds__(kBPThreads) bp_kernel(BPParams bp, const __grid_constant__ BPMaps maps,
                                                         int n0, int n_chunk,
                                                         const float* __restrict__ spad,
-                                                        cudaTextureObject_t tex,
-                                                        float* __restrict__ out, int accumulate) {
-  bp_columns<kSrc, kZAff, ZC>(bp, ParamMaps{&maps}, n0, n_chunk, spad, tex, out, accumulate,
+                                                        cudaTextureObject_t tex, BPOut dst) {
+  bp_columns<kSrc, kZAff, ZC>(bp, ParamMaps{&maps}, n0, n_chunk, spad, tex, dst,
                               (int)blockIdx.x, (int)blockIdx.y);
 }
 
@@ -260,32 +282,35 @@ static int bp_zc(BlocksFor blocks_for) {
 template <int kSrc, bool kZAff>
 static void launch_bp_zc(int zc, dim3 grid, cudaStream_t st, const BPParams& bp,
                          const BPMaps& maps, int n0, int cnt, const float* sp,
-                         cudaTextureObject_t tx, float* ob, int acc) {
+                         cudaTextureObject_t tx, const BPOut& dst) {
   if (zc == 8)
-    bp_kernel<kSrc, kZAff, 8><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, ob, acc);
+    bp_kernel<kSrc, kZAff, 8><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, dst);
   else if (zc == 4)
-    bp_kernel<kSrc, kZAff, 4><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, ob, acc);
+    bp_kernel<kSrc, kZAff, 4><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, dst);
   else
-    bp_kernel<kSrc, kZAff, 2><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, ob, acc);
+    bp_kernel<kSrc, kZAff, 2><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, dst);
+}
+
+template <int kSrc>
+static void launch_bp_src(bool zaff, int zc, dim3 grid, cudaStream_t st, const BPParams& bp,
+                          const BPMaps& maps, int n0, int cnt, const float* sp,
+                          cudaTextureObject_t tx, const BPOut& dst) {
+  if (zaff) launch_bp_zc<kSrc, true>(zc, grid, st, bp, maps, n0, cnt, sp, tx, dst);
+  else launch_bp_zc<kSrc, false>(zc, grid, st, bp, maps, n0, cnt, sp, tx, dst);
 }
 
 static void launch_bp(int src, bool zaff, int zc, dim3 grid, cudaStream_t st, const BPParams& bp,
                       const BPMaps& maps, int n0, int cnt, const float* sp, cudaTextureObject_t tx,
-                      float* ob, int acc) {
-  if (src == kSrcTex) {
-    if (zaff) launch_bp_zc<kSrcTex, true>(zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
-    else launch_bp_zc<kSrcTex, false>(zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
-  } else if (src == kSrcQuad) {
-    if (zaff) launch_bp_zc<kSrcQuad, true>(zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
-    else launch_bp_zc<kSrcQuad, false>(zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
-  } else {
-    if (zaff) launch_bp_zc<kSrcSoft, true>(zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
-    else launch_bp_zc<kSrcSoft, false>(zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
+                      const BPOut& dst) {
+  switch (src) {
+    case kSrcTex: launch_bp_src<kSrcTex>(zaff, zc, grid, st, bp, maps, n0, cnt, sp, tx, dst); break;
+    case kSrcQuad: launch_bp_src<kSrcQuad>(zaff, zc, grid, st, bp, maps, n0, cnt, sp, tx, dst); break;
+    case kSrcBoth: launch_bp_src<kSrcBoth>(zaff, zc, grid, st, bp, maps, n0, cnt, sp, tx, dst); break;
+    default: launch_bp_src<kSrcSoft>(zaff, zc, grid, st, bp, maps, n0, cnt, sp, tx, dst); break;
   }
 }
 
-int backward_impl(Plan* p, const float* sino, int batch, float* out, int accumulate,
-                  cudaStream_t st) {
+static BPParams plan_bp_params(const Plan* p) {
   const GeomParams& gp = p->gp;
   BPParams bp;
   bp.nx = gp.nx; bp.ny = gp.ny; bp.nz = gp.nz;
@@ -295,47 +320,104 @@ int backward_impl(Plan* p, const float* sino, int batch, float* out, int accumul
   bp.scale = (float)gp.bp_scale;
   bp.sino_pad_elems = (int64_t)(gp.nu + 2 * kPad) * (gp.nv + 2 * kPad);
   bp.warp = p->bp_warp;
-  const bool tex = p->sino_tex != nullptr;  // allocated for the texture plans
-  const bool quad = p->d_sino_quad != nullptr;  // the exact plans
+  return bp;
+}
+
+// Copies one batch item's sinogram into the plan's staged form: the layered
+// texture (texture plans), the quad records (exact plans) or the padded array.
+static int stage_sino(Plan* p, const float* sino, cudaStream_t st) {
+  const GeomParams& gp = p->gp;
+  if (p->sino_tex != nullptr) {
+    cudaMemcpy3DParms cp;
+    memset(&cp, 0, sizeof(cp));
+    cp.srcPtr = make_cudaPitchedPtr((void*)sino, gp.nu * sizeof(float), gp.nu, gp.nv);
+    cp.dstArray = p->sino_arrays[0];
+    cp.extent = make_cudaExtent(gp.nu, gp.nv, gp.n_views);
+    cp.kind = cudaMemcpyDeviceToDevice;
+    DTV_CUDA_TRY(cudaMemcpy3DAsync(&cp, st));
+  } else if (p->d_sino_quad != nullptr) {
+    dim3 qg((gp.nu + 1 + 31) / 32, (gp.nv + 1 + 7) / 8, gp.n_views);
+    stage_sino_quad_kernel<<<qg, 256, 0, st>>>(sino, p->d_sino_quad, gp.nu, gp.nv, gp.n_views);
+    note_launch();
+    DTV_LAUNCH_CHECK();
+  } else {
+    const int64_t per_item = (int64_t)gp.nu * gp.nv * gp.n_views;
+    stage_sino_pad_kernel<<<(int)std::min<int64_t>((per_item + 255) / 256, 148 * 16), 256, 0,
+                            st>>>(sino, p->d_sino_pad, gp.nu, gp.nv, gp.n_views);
+    note_launch();
+    DTV_LAUNCH_CHECK();
+  }
+  return DTV_OK;
+}
+
+static dim3 bp_grid(const GeomParams& gp, int* zc_out) {
   const int tiles = ((gp.nx + kBPTile - 1) / kBPTile) * ((gp.ny + kBPTile - 1) / kBPTile);
   const int zc = bp_zc([&](int c) { return (int64_t)tiles * ((gp.nz + c - 1) / c); });
-  dim3 grid(tiles, (gp.nz + zc - 1) / zc);
-  const int64_t per_item = (int64_t)gp.nu * gp.nv * gp.n_views;
+  *zc_out = zc;
+  return dim3(tiles, (gp.nz + zc - 1) / zc);
+}
+
+// The views in chunks of kBPParamViews (their maps travel in the launch
+// parameters); later chunks add onto the first one's result.
+static int bp_view_chunks(const Plan* p, int src, const float* sp, cudaTextureObject_t tx,
+                          BPOut dst, cudaStream_t st) {
+  const GeomParams& gp = p->gp;
+  const BPParams bp = plan_bp_params(p);
+  int zc;
+  const dim3 grid = bp_grid(gp, &zc);
   BPMaps maps;
-  for (int b = 0; b < batch; ++b) {
-    if (tex) {
-      cudaMemcpy3DParms cp;
-      memset(&cp, 0, sizeof(cp));
-      cp.srcPtr = make_cudaPitchedPtr((void*)(sino + b * per_item), gp.nu * sizeof(float), gp.nu,
-                                      gp.nv);
-      cp.dstArray = p->sino_arrays[0];
-      cp.extent = make_cudaExtent(gp.nu, gp.nv, gp.n_views);
-      cp.kind = cudaMemcpyDeviceToDevice;
-      DTV_CUDA_TRY(cudaMemcpy3DAsync(&cp, st));
-    } else if (quad) {
-      dim3 qg((gp.nu + 1 + 31) / 32, (gp.nv + 1 + 7) / 8, gp.n_views);
-      stage_sino_quad_kernel<<<qg, 256, 0, st>>>(sino + b * per_item, p->d_sino_quad, gp.nu,
-                                                 gp.nv, gp.n_views); note_launch();
-      DTV_LAUNCH_CHECK();
-    } else {
-      stage_sino_pad_kernel<<<(int)std::min<int64_t>((per_item + 255) / 256, 148 * 16), 256, 0,
-                              st>>>(sino + b * per_item, p->d_sino_pad, gp.nu, gp.nv, gp.n_views); note_launch();
-      DTV_LAUNCH_CHECK();
+  for (int n0 = 0; n0 < gp.n_views; n0 += kBPParamViews) {
+    const int cnt = std::min(kBPParamViews, gp.n_views - n0);
+    for (int j = 0; j < cnt; ++j) memcpy(maps.m[j], p->h_bpv[n0 + j].m, sizeof(maps.m[j]));
+    if (n0 > 0) {
+      dst.base = dst.out;
+      dst.diff_base = dst.diff;
     }
-    float* ob = out + (int64_t)b * gp.nx * gp.ny * gp.nz;
+    launch_bp(src, p->bp_zaffine != 0, zc, grid, st, bp, maps, n0, cnt, sp, tx, dst);
+    note_launch();
+    DTV_LAUNCH_CHECK();
+  }
+  return DTV_OK;
+}
+
+int backward_impl(Plan* p, const float* sino, int batch, const float* base, float* out,
+                  cudaStream_t st) {
+  const GeomParams& gp = p->gp;
+  const bool tex = p->sino_tex != nullptr;      // allocated for the texture plans
+  const bool quad = p->d_sino_quad != nullptr;  // the exact plans
+  const int64_t per_item = (int64_t)gp.nu * gp.nv * gp.n_views;
+  const int64_t vox = (int64_t)gp.nx * gp.ny * gp.nz;
+  for (int b = 0; b < batch; ++b) {
+    int rc = stage_sino(p, sino + b * per_item, st);
+    if (rc) return rc;
     const cudaTextureObject_t tx = tex ? p->sino_tex[0] : 0;
     const float* sp = tex ? nullptr
                           : quad ? reinterpret_cast<const float*>(p->d_sino_quad) : p->d_sino_pad;
     const int src = tex ? kSrcTex : quad ? kSrcQuad : kSrcSoft;
-    // views in chunks of kBPParamViews; later chunks accumulate
-    for (int n0 = 0; n0 < gp.n_views; n0 += kBPParamViews) {
-      const int cnt = std::min(kBPParamViews, gp.n_views - n0);
-      for (int j = 0; j < cnt; ++j) memcpy(maps.m[j], p->h_bpv[n0 + j].m, sizeof(maps.m[j]));
-      const int acc = n0 > 0 ? 1 : accumulate;
-      launch_bp(src, p->bp_zaffine != 0, zc, grid, st, bp, maps, n0, cnt, sp, tx, ob, acc);
-      note_launch();
-      DTV_LAUNCH_CHECK();
-    }
+    rc = bp_view_chunks(p, src, sp, tx, BPOut{out + b * vox, base ? base + b * vox : nullptr,
+                                              nullptr, nullptr}, st);
+    if (rc) return rc;
+  }
+  return DTV_OK;
+}
+
+// The correction pass of a texture plan `fast` against an exact plan `exact`
+// of the same geometry: out = BP_exact(sino), e_b = out - BP_fast(sino), one
+// launch reading both plans' staged copies of the sinogram.
+int backward_refresh_impl(Plan* fast, Plan* exact, const float* sino, int batch, float* out,
+                          float* e_b, cudaStream_t st) {
+  const GeomParams& gp = fast->gp;
+  const int64_t per_item = (int64_t)gp.nu * gp.nv * gp.n_views;
+  const int64_t vox = (int64_t)gp.nx * gp.ny * gp.nz;
+  for (int b = 0; b < batch; ++b) {
+    int rc = stage_sino(fast, sino + b * per_item, st);
+    if (rc) return rc;
+    rc = stage_sino(exact, sino + b * per_item, st);
+    if (rc) return rc;
+    rc = bp_view_chunks(fast, kSrcBoth, reinterpret_cast<const float*>(exact->d_sino_quad),
+                        fast->sino_tex[0], BPOut{out + b * vox, nullptr, e_b + b * vox, nullptr},
+                        st);
+    if (rc) return rc;
   }
   return DTV_OK;
 }
@@ -368,12 +450,13 @@ __global__ void __launch_bounds__(kBPThreads) bp_many_kernel(const __grid_consta
   const BPManyItem& it = m.it[k];
   const int local = (int)blockIdx.x - it.block0;
   const int tile = local % it.tiles, zc = local / it.tiles;
+  const BPOut dst{it.out, accumulate ? it.out : nullptr, nullptr, nullptr};
   if (it.zaffine)
     bp_columns<kSrcTex, true, ZC>(it.bp, TableMaps{it.views}, 0, it.bp.n_views, nullptr, it.tex,
-                               it.out, accumulate, tile, zc);
+                                  dst, tile, zc);
   else
     bp_columns<kSrcTex, false, ZC>(it.bp, TableMaps{it.views}, 0, it.bp.n_views, nullptr, it.tex,
-                                it.out, accumulate, tile, zc);
+                                   dst, tile, zc);
 }
 
 int backward_many_impl(Plan* const* plans, const float* const* sinos, float* const* outs, int count,

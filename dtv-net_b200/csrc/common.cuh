@@ -170,6 +170,7 @@ struct Plan {
   float4* d_cells;
   int adjoint_method;  // DTV_TUNE_ADJOINT
   double fp_samples;  // per volume, < 0 until computed
+  uint64_t geom_key;  // hash of the geometry and its per-view tables
 };
 
 constexpr int kNumRayTiles = 8;  // forward-projector ray tiles (DTV_TUNE_FP_RAY_TILE)
@@ -182,8 +183,15 @@ constexpr int kPad = 2;  // zero border of the staged volume
 // kernels entry points used across units
 int forward_impl(Plan* p, const void* vol, int vol_dtype, int batch, float* out, int epilogue,
                  const float* g, float sigma, double* abs_sum, cudaStream_t st);
-int backward_impl(Plan* p, const float* sino, int batch, float* out, int accumulate,
+// out = base + BP(sino); base NULL: out = BP(sino) (base may be out)
+int backward_impl(Plan* p, const float* sino, int batch, const float* base, float* out,
                   cudaStream_t st);
+// the correction passes of a texture-filtered plan against an exact one
+int forward_refresh_impl(Plan* fast, Plan* exact, const void* vol, int vol_dtype, int batch,
+                         const float* g, float sigma, float* w, float* g_eff, double* abs_sum,
+                         cudaStream_t st);
+int backward_refresh_impl(Plan* fast, Plan* exact, const float* sino, int batch, float* out,
+                          float* e_b, cudaStream_t st);
 int adjoint_impl(Plan* p, const float* sino, int batch, float* out, cudaStream_t st);
 int encode_pair_maps(Plan* p);
 // several plans' projections in one launch (forward.cu, backward.cu)

@@ -84,6 +84,31 @@ int make_tex3d(cudaArray_t arr, int filter_linear, cudaTextureObject_t* out) {
   return DTV_OK;
 }
 
+
+// FNV-1a over the plan's geometry: sizes, rules and spacings field by field,
+// then the per-view tables (fully initialised, no padding bytes left unset).
+static uint64_t fnv1a(const void* data, size_t n, uint64_t h) {
+  const unsigned char* b = static_cast<const unsigned char*>(data);
+  for (size_t i = 0; i < n; ++i) {
+    h ^= b[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+static uint64_t geometry_key(const GeomParams& gp, const std::vector<FPView>& fpv,
+                             const std::vector<BPView>& bpv) {
+  const int ints[9] = {gp.nx, gp.ny, gp.nz, gp.nu, gp.nv, gp.n_views, gp.phase, gp.bp_power,
+                       gp.bp_extent};
+  const double dbl[13] = {gp.voxel[0], gp.voxel[1], gp.voxel[2], gp.vol_offset[0],
+                          gp.vol_offset[1], gp.vol_offset[2], gp.det_offset[0],
+                          gp.det_offset[1], gp.step, gp.scale, gp.bp_scale, 0.0, 0.0};
+  uint64_t h = 14695981039346656037ull;
+  h = fnv1a(ints, sizeof(ints), h);
+  h = fnv1a(dbl, sizeof(dbl), h);
+  h = fnv1a(fpv.data(), sizeof(FPView) * fpv.size(), h);
+  return fnv1a(bpv.data(), sizeof(BPView) * bpv.size(), h);
+}
+
 int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Plan** out) {
   DTV_CHECK(out != nullptr, "out is NULL");
   *out = nullptr;
@@ -124,6 +149,7 @@ int create_plan(const dtv_geometry* g, int max_batch, int flags, int device, Pla
     return rc;
   }
   const GeomParams& gp = p->gp;
+  p->geom_key = geometry_key(gp, fpv, bpv);
   p->bp_zaffine = 1;
   for (int n = 0; n < gp.n_views; ++n)
     if (bpv[n].m[2] != 0.f || bpv[n].m[10] != 0.f) p->bp_zaffine = 0;
@@ -442,7 +468,58 @@ int dtv_backward(dtv_plan* plan, const float* sino, int32_t batch, float* out, i
   DTV_CHECK(sino && out, "NULL sinogram or output");
   Plan* p = reinterpret_cast<Plan*>(plan);
   DeviceGuard dg(p->device);
-  return backward_impl(p, sino, batch, out, accumulate, as_stream(stream));
+  return backward_impl(p, sino, batch, accumulate ? out : nullptr, out, as_stream(stream));
+}
+
+int dtv_backward_onto(dtv_plan* plan, const float* sino, int32_t batch, const float* base,
+                      float* out, void* stream) {
+  int rc = check_plan_call(plan, batch);
+  if (rc) return rc;
+  DTV_CHECK(sino && base && out, "NULL sinogram, base or output");
+  Plan* p = reinterpret_cast<Plan*>(plan);
+  DeviceGuard dg(p->device);
+  return backward_impl(p, sino, batch, base, out, as_stream(stream));
+}
+
+// A texture-filtered z-pair plan and an exact-weight plan of one geometry.
+static int check_refresh_pair(dtv_plan* fast, dtv_plan* exact, int batch) {
+  int rc = check_plan_call(fast, batch);
+  if (rc) return rc;
+  rc = check_plan_call(exact, batch);
+  if (rc) return rc;
+  const Plan* f = reinterpret_cast<const Plan*>(fast);
+  const Plan* e = reinterpret_cast<const Plan*>(exact);
+  DTV_CHECK((f->flags & DTV_PLAN_TEX_PAIRS) && !(f->flags & DTV_PLAN_TMA),
+            "the fast plan must be a DTV_PLAN_TEX_PAIRS plan without DTV_PLAN_TMA");
+  DTV_CHECK(e->flags & DTV_PLAN_PAIRS_EXACT, "the exact plan must be a DTV_PLAN_PAIRS_EXACT plan");
+  DTV_CHECK(f->device == e->device, "the plans are on different devices");
+  DTV_CHECK(f->geom_key == e->geom_key, "the plans' geometries differ");
+  return DTV_OK;
+}
+
+int dtv_pdhg_forward_refresh(dtv_plan* fast, dtv_plan* exact, const void* vol, int32_t vol_dtype,
+                             int32_t batch, const float* g, float sigma, float* w, float* g_eff,
+                             double* abs_sum, void* stream) {
+  int rc = check_refresh_pair(fast, exact, batch);
+  if (rc) return rc;
+  DTV_CHECK(vol && g && w && g_eff, "NULL volume, data, dual or corrected data");
+  DTV_CHECK(dtype_ok(vol_dtype), "bad volume dtype %d", vol_dtype);
+  Plan* f = reinterpret_cast<Plan*>(fast);
+  DeviceGuard dg(f->device);
+  return forward_refresh_impl(f, reinterpret_cast<Plan*>(exact), vol, vol_dtype, batch, g, sigma,
+                              w, g_eff, abs_sum, as_stream(stream));
+}
+
+int dtv_backward_refresh(dtv_plan* fast, dtv_plan* exact, const float* sino, int32_t batch,
+                         float* out, float* e_b, void* stream) {
+  int rc = check_refresh_pair(fast, exact, batch);
+  if (rc) return rc;
+  DTV_CHECK(sino && out && e_b, "NULL sinogram, output or difference");
+  DTV_CHECK(out != e_b, "out and e_b must be different buffers");
+  Plan* f = reinterpret_cast<Plan*>(fast);
+  DeviceGuard dg(f->device);
+  return backward_refresh_impl(f, reinterpret_cast<Plan*>(exact), sino, batch, out, e_b,
+                               as_stream(stream));
 }
 
 int dtv_forward_many(dtv_plan* const* plans, const void* const* vols, int32_t vol_dtype,
@@ -509,7 +586,7 @@ static int one_shot(const dtv_geometry* g, int batch, int device, int fwd, const
   {
     DeviceGuard dg(device);
     rc = fwd ? forward_impl(p, in, DTV_F32, batch, out, DTV_EPI_STORE, nullptr, 0.f, nullptr, st)
-             : backward_impl(p, in, batch, out, 0, st);
+             : backward_impl(p, in, batch, nullptr, out, st);
     cudaError_t e = cudaStreamSynchronize(st);
     if (!rc && e != cudaSuccess) rc = fail(DTV_ERR_CUDA, "sync: %s", cudaGetErrorString(e));
   }

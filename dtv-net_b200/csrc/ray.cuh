@@ -174,6 +174,45 @@ __device__ __forceinline__ float ray_sum(const Sampler& smp, const RaySetup& rs)
   return a0 + a1;
 }
 
+// Two samplers along the same ray in one loop (their set-ups differ only in
+// the coordinate offsets, so the counts agree). Each sum is accumulated in
+// exactly the order of ray_sum, so it has ray_sum's bits.
+template <class SA, class SB>
+__device__ __forceinline__ void ray_sum2(const SA& sa, const RaySetup& ra, const SB& sb,
+                                         const RaySetup& rb, float& sum_a, float& sum_b) {
+  float a0 = 0.f, a1 = 0.f, b0 = 0.f, b1 = 0.f;
+  int k = 0;
+  float kb = 0.f;
+  for (; k + 3 < ra.count; k += 4, kb += 4.f) {
+    float s[4], t[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float kf = kb + (float)j;
+      s[j] = sa(fmaf(kf, ra.dp[0], ra.p0[0]), fmaf(kf, ra.dp[1], ra.p0[1]),
+                fmaf(kf, ra.dp[2], ra.p0[2]));
+      t[j] = sb(fmaf(kf, rb.dp[0], rb.p0[0]), fmaf(kf, rb.dp[1], rb.p0[1]),
+                fmaf(kf, rb.dp[2], rb.p0[2]));
+    }
+    a0 += s[0];
+    a1 += s[1];
+    a0 += s[2];
+    a1 += s[3];
+    b0 += t[0];
+    b1 += t[1];
+    b0 += t[2];
+    b1 += t[3];
+  }
+  for (; k < ra.count; ++k) {
+    const float kf = (float)k;
+    a0 += sa(fmaf(kf, ra.dp[0], ra.p0[0]), fmaf(kf, ra.dp[1], ra.p0[1]),
+             fmaf(kf, ra.dp[2], ra.p0[2]));
+    b0 += sb(fmaf(kf, rb.dp[0], rb.p0[0]), fmaf(kf, rb.dp[1], rb.p0[1]),
+             fmaf(kf, rb.dp[2], rb.p0[2]));
+  }
+  sum_a = a0 + a1;
+  sum_b = b0 + b1;
+}
+
 // z-pair sampler through the texture unit: layer L of the half2 layered
 // texture holds (f[L-2], f[L-1]). x, y arrive as texture coordinates (shifted
 // by 1/2), z as a voxel index.

@@ -5,7 +5,8 @@ of include/dtv_b200.h; this package is its host side. There is no CPU path.
 """
 from . import _lib, autotune
 from ._lib import DtvError
-from .geometry import Geometry, Plan, backward_many, circular, forward_many, standard, vector
+from .geometry import (Geometry, Plan, backward_many, backward_refresh, circular, forward_many,
+                       forward_refresh, standard, vector)
 from .ops import (BeijingGeometry, BeijingGeometryWithFBP, Projector, RampFilter,
                   StandardGeometry, StandardGeometryWithFBP, fbp_filter, make_functions)
 from .tv import diff, diff_abs_sums, l1ball
@@ -16,7 +17,7 @@ __all__ = [
     "StandardGeometry", "StandardGeometryWithFBP", "BeijingGeometry", "BeijingGeometryWithFBP",
     "RampFilter", "fbp_filter", "make_functions", "diff",
     "diff_abs_sums", "l1ball", "DTVCP", "FISTA", "DTVFISTA", "ASDPOCS", "Batched", "BatchedFISTA",
-    "power_norm", "forward_many", "backward_many",
+    "power_norm", "forward_many", "backward_many", "forward_refresh", "backward_refresh",
     "library_path",
 ]
 

@@ -87,6 +87,9 @@ SIGNATURES = {
     "dtv_forward": [_P, _P, _I, _I, _P, _I, _P, _F, _P, _P],
     "dtv_backward": [_P, _P, _I, _P, _I, _P],
     "dtv_backward_adjoint": [_P, _P, _I, _P, _P],
+    "dtv_backward_onto": [_P, _P, _I, _P, _P, _P],
+    "dtv_pdhg_forward_refresh": [_P, _P, _P, _I, _I, _P, _F, _P, _P, _P, _P],
+    "dtv_backward_refresh": [_P, _P, _P, _I, _P, _P, _P],
     "dtv_standard_forward": [_P, _I, _FP, _I, _IP, _IP, _F, _F, _I, _P, _P],
     "dtv_standard_backward": [_P, _I, _FP, _I, _IP, _IP, _F, _F, _I, _P, _P],
     "dtv_vector_forward": [_P, _I, _IP, _IP, _FP, _I, _I, _P, _P],

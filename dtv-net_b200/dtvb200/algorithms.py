@@ -24,7 +24,8 @@ import torch
 
 from . import _lib
 from ._lib import call
-from .geometry import Plan, _ptr, _stream, backward_many, check_input, forward_many
+from .geometry import (Plan, _ptr, _stream, backward_many, backward_refresh, check_input,
+                       forward_many, forward_refresh)
 
 _FDT = {torch.float32: _lib.DTV_F32, torch.float16: _lib.DTV_F16, torch.bfloat16: _lib.DTV_BF16}
 
@@ -171,6 +172,7 @@ class DTVCP(_Graphable):
                                           int(correct_bp_every) < 1):
                 raise ValueError("correction intervals must be at least 1")
         self.exact = exact
+        self.unfused = False  # True: the correction passes as separate launches
         self.correct_every = int(correct_every)
         self.correct_bp_every = int(correct_bp_every) if correct_bp_every else int(correct_every)
         self.plan = plan
@@ -194,6 +196,13 @@ class DTVCP(_Graphable):
                                      device=plan.device) for a in range(3))
         L = 10e6
         return cls(plan, cascades, sigma=1.0 / L, tau=1.0 / L, mu=normH / 1.0, v=v, **kw)
+
+    def _fused(self) -> bool:
+        """Whether the correction passes run as one launch per operator
+        (a "pairs" plan corrected by an "exact" plan) or as separate
+        projections and element-wise steps (any other pairing)."""
+        return (self.exact is not None and self.plan.sampler == "pairs"
+                and self.exact.sampler == "exact" and not self.unfused)
 
     def _params(self):
         p = _lib.dtv_pdhg_params()
@@ -225,9 +234,10 @@ class DTVCP(_Graphable):
                               device=dev),
         }
         if self.exact is not None:
-            for k in ("s1", "s2", "g_eff"):
+            fused = self._fused()
+            for k in ("g_eff",) if fused else ("s1", "s2", "g_eff"):
                 st[k] = torch.empty(plan.sino_shape(b), dtype=torch.float32, device=dev)
-            for k in ("e_b", "t_vol"):
+            for k in ("e_b",) if fused else ("e_b", "t_vol"):
                 st[k] = torch.empty(vs, dtype=torch.float32, device=dev)
         return st
 
@@ -250,7 +260,11 @@ class DTVCP(_Graphable):
                      _ptr(st["t"]), stream)
             ex = self.exact
             refresh = ex is not None and it % self.correct_every == 0
-            if refresh:
+            if refresh and self._fused():
+                # one launch: both projections, g + e_F and the exact dual step
+                forward_refresh(plan, ex, fbar, st["g"], st["w"], st["g_eff"], self.sigma,
+                                st["loss"][it:it + 1])
+            elif refresh:
                 ns = st["w"].numel()
                 ex.forward(fbar, out=st["s1"])
                 plan.forward(fbar, out=st["s2"], epilogue=_lib.DTV_EPI_RESIDUAL, g=st["s1"])
@@ -268,14 +282,15 @@ class DTVCP(_Graphable):
                     plan.backward(st["w"], out=st["recon"])
                 elif self.correct_bp_every == 1:
                     ex.backward(st["w"], out=st["recon"])
+                elif bp_refresh and self._fused():
+                    backward_refresh(plan, ex, st["w"], st["recon"], st["e_b"])
                 elif bp_refresh:
                     ex.backward(st["w"], out=st["recon"])
                     plan.backward(st["w"], out=st["t_vol"])
                     call("dtv_lincomb", _ptr(st["recon"]), 1.0, _ptr(st["t_vol"]), -1.0,
                          _ptr(st["e_b"]), st["recon"].numel(), stream)
                 else:
-                    st["recon"].copy_(st["e_b"])
-                    plan.backward(st["w"], out=st["recon"], accumulate=True)
+                    plan.backward(st["w"], out=st["recon"], base=st["e_b"])
             else:
                 plan.adjoint(st["w"], out=st["recon"])
             call("dtv_pdhg_dual", _ptr(fbar), _ptr(st["p"]), _ptr(st["q"]), _ptr(st["s"]),
@@ -288,7 +303,7 @@ class DTVCP(_Graphable):
     def _prepare(self, image, sino):
         check_input(image, "image", self.plan.vol_shape(image.shape[0]),
                     dtypes=(torch.float32, torch.float16, torch.bfloat16))
-        key = (tuple(image.shape), image.device.index)
+        key = (tuple(image.shape), image.device.index, self._fused())
         st = self.__dict__.setdefault("_state", {}).get(key)
         if st is None:
             st = self._alloc(image)

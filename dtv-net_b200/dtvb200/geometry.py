@@ -242,8 +242,10 @@ class Plan:
         return out
 
     def backward(self, sino: torch.Tensor, out: torch.Tensor = None,
-                 accumulate: bool = False) -> torch.Tensor:
-        """FDK-weighted voxel-driven backprojection [B,1,N,H,W] -> [B,1,Z,Y,X]."""
+                 accumulate: bool = False, base: torch.Tensor = None) -> torch.Tensor:
+        """FDK-weighted voxel-driven backprojection [B,1,N,H,W] -> [B,1,Z,Y,X].
+        ``accumulate`` adds it to out; ``base`` (volume shaped, may be out)
+        gives out = base + BP(sino)."""
         check_input(sino, "sino")
         b = self._batch_of(sino, int(np.prod(self.sino_shape(1))))
         shape = self.vol_shape(b)
@@ -251,6 +253,11 @@ class Plan:
             out = torch.empty(shape, device=sino.device, dtype=torch.float32)
             accumulate = False
         check_input(out, "out", shape)
+        if base is not None:
+            check_input(base, "base", shape)
+            call("dtv_backward_onto", self._h, _ptr(sino), b, _ptr(base), _ptr(out),
+                 _stream(sino.device))
+            return out
         call("dtv_backward", self._h, _ptr(sino), b, _ptr(out), int(bool(accumulate)),
              _stream(sino.device))
         return out
@@ -280,6 +287,38 @@ class Plan:
 
 def _ptr_array(ts):
     return (ctypes.c_void_p * len(ts))(*[t.data_ptr() for t in ts])
+
+
+def forward_refresh(fast: Plan, exact: Plan, vol: torch.Tensor, g: torch.Tensor,
+                    w: torch.Tensor, g_eff: torch.Tensor, sigma: float,
+                    abs_sum: torch.Tensor = None):
+    """The correction pass of a texture-filtered z-pair plan ``fast``
+    (sampler "pairs") against the exact-weight plan ``exact`` (sampler
+    "exact") of the same geometry, in one launch: with e and a the exact and
+    fast projections of vol, g_eff = g + (a - e) and
+    w = (w + sigma (e - g)) / (1 + sigma); abs_sum += sum|e - g|."""
+    check_input(vol, "volume", dtypes=tuple(_DT))
+    b = fast._batch_of(vol, int(np.prod(fast.vol_shape(1))))
+    shape = fast.sino_shape(b)
+    for t, n in ((g, "g"), (w, "w"), (g_eff, "g_eff")):
+        check_input(t, n, shape)
+    if abs_sum is not None:
+        check_input(abs_sum, "abs_sum", dtypes=(torch.float64,))
+    call("dtv_pdhg_forward_refresh", fast._h, exact._h, _ptr(vol), _DT[vol.dtype], b, _ptr(g),
+         float(sigma), _ptr(w), _ptr(g_eff), _ptr(abs_sum), _stream(vol.device))
+
+
+def backward_refresh(fast: Plan, exact: Plan, sino: torch.Tensor, out: torch.Tensor,
+                     e_b: torch.Tensor):
+    """out = exact.backward(sino), e_b = out - fast.backward(sino), in one
+    launch (the plans as for forward_refresh)."""
+    check_input(sino, "sino")
+    b = fast._batch_of(sino, int(np.prod(fast.sino_shape(1))))
+    shape = fast.vol_shape(b)
+    check_input(out, "out", shape)
+    check_input(e_b, "e_b", shape)
+    call("dtv_backward_refresh", fast._h, exact._h, _ptr(sino), b, _ptr(out), _ptr(e_b),
+         _stream(sino.device))
 
 
 def forward_many(plans, vols, outs=None, epilogue: int = 0, gs=None, sigma: float = 0.0):

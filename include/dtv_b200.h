@@ -265,6 +265,34 @@ DTV_API int dtv_forward(dtv_plan* plan, const void* vol, int32_t vol_dtype, int3
  * accumulated into when accumulate != 0. */
 DTV_API int dtv_backward(dtv_plan* plan, const float* sino, int32_t batch, float* out, int32_t accumulate,
                  void* stream);
+/* out = base + BP(sino), same backprojector as dtv_backward; base may equal
+ * out (then it is dtv_backward with accumulate != 0). No reference
+ * counterpart: DTVCP's corrected iterations add the stored backprojector
+ * correction this way without copying it into out first. */
+DTV_API int dtv_backward_onto(dtv_plan* plan, const float* sino, int32_t batch, const float* base,
+                              float* out, void* stream);
+
+/* The correction passes of a texture-filtered z-pair plan `fast`
+ * (DTV_PLAN_TEX_PAIRS, not DTV_PLAN_TMA) against an exact-weight plan `exact`
+ * (DTV_PLAN_PAIRS_EXACT) of the same geometry, one launch per operator that
+ * samples through both plans. No reference counterpart (the reference has
+ * one texture-filtered operator pair); the dual step is DTVCP.py:38-39.
+ *
+ * dtv_pdhg_forward_refresh: per ray, with e = E(vol) and a = A(vol) the exact
+ * and fast projections (each with the bits dtv_forward gives on its plan),
+ *   g_eff = g + (a - e),  w = (w + sigma*(e - g)) / (1 + sigma),
+ * and abs_sum[0] += sum |e - g| (device double, may be NULL). g_eff must not
+ * alias g or w.
+ *
+ * dtv_backward_refresh: out = BP_exact(sino), e_b = out - BP_fast(sino) (out
+ * and e_b distinct buffers of volume shape; above 640 views e_b adds the
+ * difference of each chunk of 640 views, a sum rounded per chunk). Plans of different geometry,
+ * sampler or device return DTV_ERR_INVALID. */
+DTV_API int dtv_pdhg_forward_refresh(dtv_plan* fast, dtv_plan* exact, const void* vol,
+                                     int32_t vol_dtype, int32_t batch, const float* g, float sigma,
+                                     float* w, float* g_eff, double* abs_sum, void* stream);
+DTV_API int dtv_backward_refresh(dtv_plan* fast, dtv_plan* exact, const float* sino, int32_t batch,
+                                 float* out, float* e_b, void* stream);
 /* Exact transpose of dtv_forward's STORE map (same samples, same weights,
  * software sampler): out = A^T sino. No reference counterpart — the reference
  * paired forward with the FDK backprojector as its gradient

@@ -108,6 +108,10 @@ def test_null_arguments_are_rejected():
     assert L.dtv_plan_destroy(None) == 0
     assert L.dtv_diff(None, None, None, 1, 0, 0, 0, None) == 1
     assert L.dtv_l1ball(None, None, 0, None, None, None, None) == 1
+    assert L.dtv_backward_onto(None, None, 1, None, None, None) == 1
+    assert L.dtv_pdhg_forward_refresh(None, None, None, 0, 1, None, 0.0, None, None, None,
+                                      None) == 1
+    assert L.dtv_backward_refresh(None, None, None, 1, None, None, None) == 1
 
 
 def test_check_input_errors():
