@@ -168,6 +168,16 @@ def dtv_params(plan, dev, iters=8):
     return dict(sigma=sigma, tau=sigma, mu=1.0, v=(0.5, 0.5, 0.5), quirk=False)
 
 
+def rel_rmse(a, b):
+    """Relative RMSE of a (tensor or array) against the reference b."""
+    import numpy as np
+    if hasattr(a, "detach"):
+        a = a.detach().double().cpu().numpy()
+    a = np.asarray(a, np.float64).reshape(-1)
+    b = np.asarray(b, np.float64).reshape(-1)
+    return float(np.sqrt(np.mean((a - b) ** 2) / np.mean(b ** 2)))
+
+
 def time_steps(fn, steps, stream):
     import torch
     start = torch.cuda.Event(enable_timing=True)
@@ -675,6 +685,28 @@ def run_batch16(args):
 
     plain_all()
     ps = time_steps(plain_all, args.steps, stream)
+
+    # checker leg (outside the timed regions): the smallest reconstruction of
+    # the batch against the FP64 oracle's FISTA on the same sinogram
+    check = None
+    if not args.no_check:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import oracle as O
+        i = min(range(16), key=lambda k: specs[k][0] * specs[k][0] * specs[k][1])
+        n, views = specs[i]
+        d = int(round(1.5 * n))
+        og = O.circular_geometry(np.linspace(0, 360, views, endpoint=False), (n, n, n),
+                                 (1.0,) * 3, (d, d), (1.5, 1.5), 500.0, 1000.0)
+        t0 = time.perf_counter()
+        fp = lambda x: O.forward(og, x).reshape(x.shape[0], 1, *og.sino_shape)  # noqa: E731
+        bp = lambda s_: O.backward(og, s_).reshape(s_.shape[0], 1, *og.vol_shape)  # noqa: E731
+        ref = O.fista_run(fp, bp, np.zeros((1, 1) + og.vol_shape),
+                          sinos[i].double().cpu().numpy(), 30, 1e-3, 0.05)
+        got = batch.run(imgs, sinos)[i]
+        check = {"reconstruction": rel_rmse(got, ref), "gate": 1e-3, "volume": [n, views],
+                 "seconds": time.perf_counter() - t0,
+                 "how": "relative RMSE of the batch's smallest reconstruction (30 FISTA "
+                        "iterations) against the FP64 oracle's FISTA on the same sinogram"}
     line = {
         "metric": METRIC, "value": units * args.steps / secs / 1e9, "unit": UNIT, "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
@@ -692,6 +724,7 @@ def run_batch16(args):
             "gpu_launches_per_run": lock.launches_per_run},
         "gpu_launches": batch.launches_per_run * args.steps,
         "clocks": clk.summary(),
+        "error_vs_fp64": check,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -836,10 +869,20 @@ def run_fista64(args):
     _, plain = build("soft", False)
     plain()
     ps = time_steps(plain, args.steps, stream)
-    cpu = None
+    cpu = check = None
     if not args.no_cpu:
-        cpu = fista64_cpu(c, truth[0, 0].double().cpu().numpy(), dtv_params(plan, dev)["sigma"],
-                          tuple(power_norm((64, 64, 64), a, False, device=dev) for a in range(3)))
+        sigma = dtv_params(plan, dev)["sigma"]
+        v = tuple(power_norm((64, 64, 64), a, False, device=dev) for a in range(3))
+        cpu, ref = fista64_cpu(c, truth[0, 0].double().cpu().numpy(), sigma, v)
+        # this library's outputs of the same step (eager, outside the timed region)
+        alg = dtvb200.DTVFISTA(plan, c["iters"], sigma=sigma, v=v, t=(1e-3,) * 3, quirk=False)
+        s_gpu = plan.forward(truth)
+        b_gpu = plan.backward(s_gpu)
+        r_gpu = alg.run(torch.zeros(plan.vol_shape(1), device=dev), s_gpu)
+        check = {"forward": rel_rmse(s_gpu, ref["sino"]), "backward": rel_rmse(b_gpu, ref["bp"]),
+                 "reconstruction": rel_rmse(r_gpu, ref["recon"]), "gate": 1e-3,
+                 "how": "relative RMSE of each output of the step against the FP64 oracle's "
+                        "run of the same step (its own FP64 projections) at full size"}
     line = {
         "metric": METRIC, "value": units * args.steps / secs / 1e9, "unit": UNIT, "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
@@ -854,6 +897,7 @@ def run_fista64(args):
         "gpu_launches": launches * args.steps,
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
+        "error_vs_fp64": check,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -873,14 +917,16 @@ def fista64_cpu(c, truth_np, sigma, v):
     bp = lambda s: O.backward(og, s).reshape(s.shape[0], 1, *og.vol_shape)  # noqa: E731
     t0 = time.perf_counter()
     sino = fp(vol.reshape(1, 1, *vol.shape))
-    bp(sino)
-    O.dtvfista_run(fp, bp, np.zeros((1, 1) + og.vol_shape), sino, (c["nx"], c["ny"], c["nz"]),
-                   c["iters"], sigma, v, (1e-3,) * 3, quirk=False)
+    bsino = bp(sino)
+    recon = O.dtvfista_run(fp, bp, np.zeros((1, 1) + og.vol_shape), sino,
+                           (c["nx"], c["ny"], c["nz"]), c["iters"], sigma, v, (1e-3,) * 3,
+                           quirk=False)
     secs = time.perf_counter() - t0
     units = (c["iters"] + 1) * (O.fp_samples(og) + c["nx"] * c["ny"] * c["nz"] * c["n_views"])
-    return {"value": units / secs / 1e9, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
-            "recon_per_s": 1.0 / secs,
-            "sample": "the whole step (FP + BP + 20 FISTA-DTV iterations), FP64 oracle, once"}
+    return ({"value": units / secs / 1e9, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+             "recon_per_s": 1.0 / secs,
+             "sample": "the whole step (FP + BP + 20 FISTA-DTV iterations), FP64 oracle, once"},
+            {"sino": sino, "bp": bsino, "recon": recon})
 
 
 def fp64_check_large(dev, sampler, K, iters):
@@ -1025,8 +1071,49 @@ def run_peaks(args):
         "atomic_v4_scattered": [L.measure_atomic_v4_rate(72 << 16, 1) for _ in range(3)],
     }
     print(json.dumps({"unit": "per second", "sm_count": torch.cuda.get_device_properties(
-        0).multi_processor_count, "rates": rates}), flush=True)
+        0).multi_processor_count, "rates": rates,
+        "projector_concurrency_ms": projector_concurrency()}), flush=True)
     return 0
+
+
+def projector_concurrency(reps=10):
+    """Whether the SM-side samplers add throughput to the texture unit: the
+    headline forward projection by the z-pair texture plan, the exact-record
+    plan (16-byte loads through L1) and the shared-memory (TMA) plan with no
+    tiles on the texture unit, each alone and two at a time on two streams
+    (ms per pair of launches; independent units would give the slower one's
+    time, a shared one the sum)."""
+    import torch
+
+    import dtvb200
+    dev = torch.device("cuda", 0)
+    c = dict(CFG)
+    geo, truth, _ = make_problem(dev, c, c["seed"])
+    P = {s: dtvb200.Plan(geo, sampler=s, device=dev) for s in ("pairs", "exact", "tma")}
+    P["tma"].set_tuning(dtvb200._lib.DTV_TUNE_FP_TEX_SHARE, 0)
+    out = {s: torch.empty(P["pairs"].sino_shape(1), device=dev) for s in P}
+    streams = [torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)]
+    main = torch.cuda.current_stream(dev)
+
+    def launch(names):
+        for st in streams:
+            st.wait_stream(main)
+        for i, s in enumerate(names):
+            with torch.cuda.stream(streams[i]):
+                P[s].forward(truth, out=out[s])
+        for st in streams:
+            main.wait_stream(st)
+
+    def timed(names):
+        for _ in range(2):
+            launch(names)
+        return time_steps(lambda: launch(names), reps, main) / reps * 1e3
+
+    res = {"+".join(v): timed(v) for v in (["pairs"], ["exact"], ["tma"], ["pairs", "exact"],
+                                           ["pairs", "tma"], ["pairs", "pairs"])}
+    for s in P.values():
+        s.close()
+    return res
 
 
 def run_profile(args):
