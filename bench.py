@@ -471,7 +471,11 @@ def run_ours(args):
     K = args.correct_every if args.sampler in ("pairs", "tex", "tma") else 0
     xplan = dtvb200.Plan(geo, max_batch=1, sampler="exact", device=dev) if K else None
     corr = dict(exact=xplan, correct_every=max(K, 1))
-    alg = dtvb200.DTVCP(plan, c["iters"], t_refresh=10, use_graph=True, **corr, **prm)
+    # the projected iterate fbar is stored in FP16 (--fbar f16) or FP32; the
+    # iterate f, the duals and all arithmetic stay FP32
+    fdt = torch.float16 if args.fbar == "f16" else torch.float32
+    alg = dtvb200.DTVCP(plan, c["iters"], t_refresh=10, use_graph=True, f_dtype=fdt, **corr,
+                        **prm)
     img = torch.zeros(plan.vol_shape(1), device=dev)
     stream = torch.cuda.current_stream(dev)
 
@@ -534,22 +538,25 @@ def run_ours(args):
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     achieved = fp_bytes / (t_fp * 1e-3) / 1e9
 
-    # ---- FP16 storage variant and the plain FP32 single-volume path
+    # ---- the other fbar storage and the plain FP32 single-volume path
     extra = {}
     if not args.no_variants:
-        ref_f = alg.run(img, sino)
-        plan16 = dtvb200.Plan(geo, max_batch=1, sampler=args.sampler, stage_f16=True, device=dev)
-        alg16 = dtvb200.DTVCP(plan16, c["iters"], t_refresh=10, use_graph=True,
-                              f_dtype=torch.float16, **corr, **prm)
-        alg16.run(img, sino)
-        s16 = time_steps(lambda: alg16.run(img, sino), args.steps, stream)
-        f16 = alg16.run(img, sino)
-        err16 = float(torch.sqrt(((f16 - ref_f).double() ** 2).mean() / (ref_f.double() ** 2).mean()))
+        f_head = alg.run(img, sino)
+        odt = torch.float32 if fdt == torch.float16 else torch.float16
+        alt = dtvb200.DTVCP(plan, c["iters"], t_refresh=10, use_graph=True, f_dtype=odt, **corr,
+                            **prm)
+        alt.run(img, sino)
+        s_alt = time_steps(lambda: alt.run(img, sino), args.steps, stream)
+        f_alt = alt.run(img, sino)
+        f32_ref, other = (f_alt, f_head) if odt == torch.float32 else (f_head, f_alt)
+        err16 = float(torch.sqrt(((other - f32_ref).double() ** 2).mean()
+                                 / (f32_ref.double() ** 2).mean()))
         extra = {
-            "fp16_storage": {"value": units * args.steps / s16 / 1e9,
-                             "recon_per_s": args.steps / s16,
-                             "rel_rmse_vs_fp32_storage": err16},
+            ("fp32_fbar_storage" if odt == torch.float32 else "fp16_fbar_storage"): {
+                "value": units * args.steps / s_alt / 1e9, "recon_per_s": args.steps / s_alt},
+            "rel_rmse_fp16_vs_fp32_fbar_storage": err16,
         }
+        del alt
         # the plain FP32 single-volume path: FP32 staging and FP32 weights,
         # one launch per operator, no graph ("soft"); and the same through an
         # FP32 3-D texture, as the reference samples ("tex")
@@ -585,8 +592,9 @@ def run_ours(args):
         "config": {"workload": workload_name(c), "parallelism": f"replicas x{ws}",
                    "sampler": args.sampler, "graph": "one CUDA graph per reconstruction",
                    "l2": "working set > L2 (volume, 4 dual volumes, sinograms ~0.5 GB)",
-                   "storage": ("f, duals, sinograms FP32; the projected volume staged as "
-                               "FP16 z-pairs; FP32 accumulation"),
+                   "storage": (f"f, duals, sinograms FP32; the projected iterate fbar stored "
+                               f"{'FP16' if args.fbar == 'f16' else 'FP32'} and staged as FP16 "
+                               f"z-pairs; FP32 accumulation"),
                    "correction": (f"operators corrected by the exact-weight plan every {K} "
                                   f"iterations (DTVCP exact=)" if K else None),
                    "inputs": "seeded ellipsoid phantom, Poisson noise"},
@@ -1141,7 +1149,8 @@ def run_profile(args):
     K = args.correct_every if args.sampler in ("pairs", "tex", "tma") else 0
     xplan = dtvb200.Plan(geo, max_batch=1, sampler="exact", device=dev) if K else None
     alg = dtvb200.DTVCP(plan, args.profile, t_refresh=10, use_graph=False, exact=xplan,
-                        correct_every=max(K, 1), **prm)
+                        correct_every=max(K, 1),
+                        f_dtype=torch.float16 if args.fbar == "f16" else torch.float32, **prm)
     f = alg.run(torch.zeros(plan.vol_shape(1), device=dev), sino)
     torch.cuda.synchronize()
     print(json.dumps({"profile_iterations": args.profile, "sampler": args.sampler,
@@ -1160,6 +1169,8 @@ def main():
     ap.add_argument("--small", action="store_true", help="64^3 smoke-size workload")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--fbar", choices=("f16", "f32"), default="f16",
+                    help="storage of DTV's projected iterate fbar (headline workload)")
     ap.add_argument("--correct-every", type=int, default=8, metavar="K",
                     help="refresh the exact-weight correction of a texture-filtered sampler "
                          "every K DTV iterations (0: uncorrected)")
