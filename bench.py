@@ -623,7 +623,21 @@ def run_ours(args):
                          "forward_achieved": fp_samples / (t_fp * 1e-3),
                          "forward_frac": fp_samples / (t_fp * 1e-3) / tex_peak,
                          "backward_achieved": V * n_views / (t_bp * 1e-3),
-                         "backward_frac": V * n_views / (t_bp * 1e-3) / tex_peak}},
+                         "backward_frac": V * n_views / (t_bp * 1e-3) / tex_peak},
+                     # secondary figures of the survey's roofline: the trilinear
+                     # tap rate (8 taps of 2-byte FP16 values per sample) and a
+                     # whole iteration's algorithmic bytes (forward as above;
+                     # single-pass backprojection P*4 + 2*V*4; DTV-PDHG update
+                     # 13*V*4 + 3*P*4) over its measured time
+                     "tap_rate_gbs": 8 * fp_samples * 2 / (t_fp * 1e-3) / 1e9,
+                     "iteration": {
+                         "algorithmic_bytes": fp_bytes + (P * 4 + 2 * V * 4)
+                                              + (13 * V * 4 + 3 * P * 4),
+                         "ms": secs / args.steps / c["iters"] * 1e3,
+                         "achieved_gbs": (fp_bytes + P * 4 + 2 * V * 4 + 13 * V * 4 + 3 * P * 4)
+                                         / (secs / args.steps / c["iters"]) / 1e9,
+                         "frac": (fp_bytes + P * 4 + 2 * V * 4 + 13 * V * 4 + 3 * P * 4)
+                                 / (secs / args.steps / c["iters"]) / 1e9 / hbm_peak}},
         "error_vs_fp64": check,
         "cpu_baseline": cpu,
         "reference_cuda_baseline": ref_cuda,
