@@ -84,13 +84,14 @@ def test_backward_onto(cuda):
     assert torch.equal(same, ref)
 
 
-@pytest.mark.parametrize("use_graph", [False, True])
-def test_dtvcp_fused_correction_equals_separate(cuda, use_graph):
+@pytest.mark.parametrize("use_graph,f_dtype", [(False, torch.float32), (True, torch.float32),
+                                               (True, torch.float16)])
+def test_dtvcp_fused_correction_equals_separate(cuda, use_graph, f_dtype):
     fast, exact = plans(cuda, n=40, views=24)
     truth = volumes(cuda, 40, 1)
     sino = fast.forward(truth)
     kw = dict(sigma=2e-3, tau=2e-3, mu=1.0, v=(0.5,) * 3, quirk=False, use_graph=use_graph,
-              exact=exact, correct_every=3)
+              exact=exact, correct_every=3, f_dtype=f_dtype)
     fused = dtvb200.DTVCP(fast, 10, **kw)
     assert fused._fused()
     sep = dtvb200.DTVCP(fast, 10, **kw)
