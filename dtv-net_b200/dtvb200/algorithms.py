@@ -384,21 +384,35 @@ class FISTA(_Graphable):
 class BatchedFISTA:
     """:class:`FISTA` on several reconstructions in lockstep: per iteration one
     forward-projector launch, one backprojector launch and one update launch
-    cover every volume, whatever their sizes and view counts
-    (dtv_forward_many, dtv_backward_many, dtv_fista_update_many). With ``use_graph`` a whole run
-    is one captured CUDA graph. The plans must be "pairs" (or "tma") plans;
-    each reconstruction gives the same result as its own :class:`FISTA` run."""
+    cover every volume of a group, whatever their sizes and view counts
+    (dtv_forward_many, dtv_backward_many, dtv_fista_update_many). ``groups``
+    splits the volumes into that many groups of about equal work, each in
+    lockstep on its own stream, so one group's backprojection runs beside
+    another's forward projection. With ``use_graph`` a whole run is one
+    captured CUDA graph. The plans must be "pairs" (or "tma") plans; each
+    reconstruction gives the same result as its own :class:`FISTA` run."""
 
     def __init__(self, plans, cascades: int = 30, lamb: float = 10e3, L: float = 0.0001,
-                 use_graph: bool = True):
+                 use_graph: bool = True, groups: int = 1):
         self.plans = list(plans)
         if len({id(p) for p in self.plans}) != len(self.plans):
             raise ValueError("each reconstruction needs a plan of its own")
+        if int(groups) < 1:
+            raise ValueError("groups must be at least 1")
         self.cascades = int(cascades)
         self.lamb, self.L = float(lamb), float(L)
         self.use_graph = use_graph
         self.launches_per_run = 0
         self._state = {}
+        # greedy balance of (rays x edge) work over the groups, heaviest first
+        work = [float(np.prod(p.sino_shape(1))) * max(p.vol_shape(1)) for p in self.plans]
+        G = min(int(groups), len(self.plans))
+        loads, self._groups = [0.0] * G, [[] for _ in range(G)]
+        for i in sorted(range(len(self.plans)), key=lambda i: -work[i]):
+            g = loads.index(min(loads))
+            self._groups[g].append(i)
+            loads[g] += work[i]
+        self._streams = None
 
     def _prepare(self, images, sinos):
         key = tuple((tuple(i.shape), i.device.index) for i in images)
@@ -417,7 +431,7 @@ class BatchedFISTA:
             d["g"].copy_(s)
         return key, st
 
-    def _enqueue(self, st):
+    def _enqueue_group(self, plans, st):
         stream = _stream(st[0]["y"].device)
         ys, rs, gs, bps = ([d[k] for d in st] for k in ("y", "r", "g", "bp"))
         vp = ctypes.c_void_p * len(st)
@@ -429,12 +443,27 @@ class BatchedFISTA:
             d["xp"].copy_(d["img"])
         t = 1.0
         for _ in range(self.cascades):
-            forward_many(self.plans, ys, rs, epilogue=_lib.DTV_EPI_RESIDUAL, gs=gs)
-            backward_many(self.plans, rs, bps)
+            forward_many(plans, ys, rs, epilogue=_lib.DTV_EPI_RESIDUAL, gs=gs)
+            backward_many(plans, rs, bps)
             tp = (1 + math.sqrt(1 + 4 * t ** 2)) / 2
             call("dtv_fista_update_many", *upd, len(st), self.L, self.lamb * self.L,
                  (t - 1) / tp, stream)
             t = tp
+
+    def _enqueue(self, st):
+        if len(self._groups) == 1:
+            self._enqueue_group(self.plans, st)
+            return
+        dev = st[0]["y"].device
+        if self._streams is None:
+            self._streams = [torch.cuda.Stream(device=dev) for _ in self._groups]
+        main = torch.cuda.current_stream(dev)
+        for idx, sm in zip(self._groups, self._streams):
+            sm.wait_stream(main)
+            with torch.cuda.stream(sm):
+                self._enqueue_group([self.plans[i] for i in idx], [st[i] for i in idx])
+        for sm in self._streams:
+            main.wait_stream(sm)
 
     def run(self, images, sinos, outs=None):
         key, st = self._prepare(images, sinos)

@@ -70,6 +70,23 @@ def test_backward_many_equals_per_plan(cuda, sampler):
         assert torch.allclose(a, 2 * o, rtol=1e-6, atol=0)
 
 
+def test_backward_many_splits_by_views(cuda):
+    """Plans whose views together exceed one launch's map budget (560 views)
+    run in several launches, and a plan with more views than that reads its
+    maps from device memory: the values are those of one plan at a time."""
+    plans = []
+    for views in (250, 250, 250, 600, 40):
+        ang = np.linspace(0, 360, views, endpoint=False)
+        plans.append(dtvb200.Plan(dtvb200.circular(ang, (16, 18, 12), (1.0,) * 3, (24, 20),
+                                                   (1.2, 1.2), 500.0, 1000.0),
+                                  sampler="pairs", device=cuda))
+    g = torch.Generator(device=cuda).manual_seed(8)
+    sinos = [torch.rand(p.sino_shape(1), device=cuda, generator=g) for p in plans]
+    outs = dtvb200.backward_many(plans, sinos)
+    for p, s_, o in zip(plans, sinos, outs):
+        assert torch.equal(o, p.backward(s_))
+
+
 def test_many_rejects_unsupported_plans(cuda):
     plans = _plans(cuda)[:3]
     vols = _vols(cuda, plans)
@@ -92,12 +109,13 @@ def test_many_rejects_unsupported_plans(cuda):
 
 
 @pytest.mark.parametrize("graph", [False, True])
-def test_batched_fista_equals_fista(cuda, graph):
+@pytest.mark.parametrize("groups", [1, 3])
+def test_batched_fista_equals_fista(cuda, graph, groups):
     plans = _plans(cuda)[:8]
     truths = _vols(cuda, plans, seed=7)
     sinos = [p.forward(t) for p, t in zip(plans, truths)]
     imgs = [torch.zeros_like(t) for t in truths]
-    batch = dtvb200.BatchedFISTA(plans, 6, lamb=0.05, L=1e-3, use_graph=graph)
+    batch = dtvb200.BatchedFISTA(plans, 6, lamb=0.05, L=1e-3, use_graph=graph, groups=groups)
     out = batch.run(imgs, sinos)
     out2 = batch.run(imgs, sinos)
     for p, i, s, o, o2 in zip(plans, imgs, sinos, out, out2):
