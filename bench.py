@@ -697,7 +697,7 @@ def run_batch16(args):
     lock = None
     if args.sampler in ("pairs", "tma"):
         lock = dtvb200.BatchedFISTA([a.plan for a in algs], 30, lamb=0.05, L=1e-3,
-                                    use_graph=True)
+                                    use_graph=True, groups=2)
         lock.run(imgs, sinos)
         ls = time_steps(lambda: lock.run(imgs, sinos), args.steps, stream)
 
@@ -743,7 +743,7 @@ def run_batch16(args):
         "speedup_vs_plain_fp32": ps / secs,
         "lockstep_one_launch_per_operator": None if lock is None else {
             "value": units * args.steps / ls / 1e9, "recon_per_s": 16 * args.steps / ls,
-            "gpu_launches_per_run": lock.launches_per_run},
+            "groups": 2, "gpu_launches_per_run": lock.launches_per_run},
         "gpu_launches": batch.launches_per_run * args.steps,
         "clocks": clk.summary(),
         "error_vs_fp64": check,
