@@ -39,7 +39,7 @@ CFG = dict(nx=256, ny=256, nz=256, voxel=1.0, nu=384, nv=384, pitch=1.2, n_views
 # utilisation of that launch, from the ncu capture summarised in
 # profiles/fp_pair_kernel_sparse_view_dtv.md (`python bench.py --profile 12`).
 # They describe the kernel as captured there, not this run.
-FP_NCU = {"pairs": {"traffic": 142.958336e6 + 26.171136e6, "tex_pipe_pct": 95.3,
+FP_NCU = {"pairs": {"traffic": 142.743040e6 + 28.150784e6, "tex_pipe_pct": 95.4,
                     "source": "profiles/fp_pair_kernel_sparse_view_dtv.md"}}
 
 # Same-FOV downsample on which the 100-iteration reconstruction is checked
