@@ -660,6 +660,134 @@ __global__ void __launch_bounds__(256, 6) pdhg_dual_kernel(const T* __restrict__
   }
 }
 
+// Four consecutive values as floats (16-byte aligned for float, 8-byte for
+// the 16-bit types).
+__device__ __forceinline__ float4 load4_as_float(const float* p, int64_t i) {
+  return __ldg(reinterpret_cast<const float4*>(p + i));
+}
+__device__ __forceinline__ float4 load4_as_float(const __half* p, int64_t i) {
+  const uint2 w = __ldg(reinterpret_cast<const uint2*>(p + i));
+  const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&w.x));
+  const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&w.y));
+  return make_float4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ float4 load4_as_float(const __nv_bfloat16* p, int64_t i) {
+  const uint2 w = __ldg(reinterpret_cast<const uint2*>(p + i));
+  const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w.x));
+  const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w.y));
+  return make_float4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ float4 f4_zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+
+// The same dual step with four consecutive x per thread: the duals move as
+// 16-byte vectors and f-bar's x-neighbours come from the thread's own vector,
+// for about a third of the instructions per voxel. For rows of a multiple of
+// 4 voxels (and, with the D_y wrap, a multiple of 4 rows: the wrapped
+// neighbour vector then stays aligned). A block of 64 x 4 threads covers
+// 256 x 4 columns and kX4ZS slices; the duals of all its slices are loaded
+// before any store, as in pdhg_dual_kernel.
+constexpr int kX4TX = 256, kX4ZS = 2;
+template <class T>
+__global__ void __launch_bounds__(256, 4) pdhg_dual_x4_kernel(const T* __restrict__ fbar,
+                                                           float* __restrict__ p,
+                                                           float* __restrict__ q,
+                                                           float* __restrict__ s,
+                                                           float* __restrict__ c, Dims d,
+                                                           float a0, float a1, float a2,
+                                                           float smu, L1Chan* chans,
+                                                           int n_tiles) {
+  __shared__ unsigned int hs[3][3 * kL1B1];
+  for (int i = ltid(); i < 9 * kL1B1; i += lthreads()) (&hs[0][0])[i] = 0u;
+  __syncthreads();
+  unsigned int kmax[3] = {0u, 0u, 0u};
+  const int tx = (d.X + kX4TX - 1) / kX4TX, ty = (d.Y + kTY - 1) / kTY;
+  const int zslabs = (d.Z + kX4ZS - 1) / kX4ZS;
+  const int64_t plane = (int64_t)d.X * d.Y;
+  const int64_t oy = axis_off(d, 1);
+  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const int bx = tile % tx, r = tile / tx;
+    const int by = r % ty, bz = r / ty;
+    const int x0 = bx * kX4TX + (int)threadIdx.x * 4, y = by * kTY + (int)threadIdx.y;
+    const int z0 = (bz % zslabs) * kX4ZS;
+    const int nz = min(kX4ZS, d.Z - z0);
+    const int64_t base = (int64_t)(bz / zslabs) * d.N;
+    const bool in = x0 < d.X && y < d.Y;
+    const int64_t i0 = ((int64_t)z0 * d.Y + y) * d.X + x0;
+    const T* fb = fbar + base;
+    float4 P[kX4ZS], Q[kX4ZS], S[kX4ZS], C[kX4ZS];
+#pragma unroll
+    for (int k = 0; k < kX4ZS; ++k) {
+      P[k] = Q[k] = S[k] = C[k] = f4_zero();
+      if (in && k < nz) {
+        const int64_t t = base + i0 + k * plane;
+        P[k] = *reinterpret_cast<const float4*>(p + t);
+        Q[k] = *reinterpret_cast<const float4*>(q + t);
+        S[k] = *reinterpret_cast<const float4*>(s + t);
+        C[k] = *reinterpret_cast<const float4*>(c + t);
+      }
+    }
+    float4 fc = in ? load4_as_float(fb, i0) : f4_zero();
+#pragma unroll
+    for (int k = 0; k < kX4ZS; ++k) {
+      if (!(in && k < nz)) continue;
+      const int64_t i = i0 + k * plane;
+      const int z = z0 + k;
+      const bool zv = z < d.Z - 1;
+      const float4 fn = zv ? load4_as_float(fb, i + plane) : f4_zero();
+      // with the wrap, i and N - Y are multiples of 4: all four share the test
+      const bool yv = d.quirk ? (i < d.N - d.Y) : (y < d.Y - 1);
+      const float4 fy = yv ? load4_as_float(fb, i + oy) : f4_zero();
+      const bool xlast = x0 + 3 < d.X - 1;  // the 4th voxel has an x-neighbour
+      const float fx4 = xlast ? load_as_float(fb, i + 4) : 0.f;
+      const float fcs[4] = {fc.x, fc.y, fc.z, fc.w};
+      const float gxs[4] = {fc.y - fc.x, fc.z - fc.y, fc.w - fc.z, xlast ? fx4 - fc.w : -fc.w};
+      const float fys[4] = {fy.x, fy.y, fy.z, fy.w};
+      const float fns[4] = {fn.x, fn.y, fn.z, fn.w};
+      const float ps[4] = {P[k].x, P[k].y, P[k].z, P[k].w};
+      const float qs[4] = {Q[k].x, Q[k].y, Q[k].z, Q[k].w};
+      const float ss[4] = {S[k].x, S[k].y, S[k].z, S[k].w};
+      const float cs[4] = {C[k].x, C[k].y, C[k].z, C[k].w};
+      float np[4], nq[4], ns[4];
+      const int64_t t = base + i;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float gy = yv ? fys[e] - fcs[e] : -fcs[e];
+        const float gz = zv ? fns[e] - fcs[e] : -fcs[e];
+        np[e] = fmaf(a0, gxs[e], ps[e]);
+        nq[e] = fmaf(a1, gy, qs[e]);
+        ns[e] = fmaf(a2, gz, ss[e]);
+        // -relu(-c - sigma*mu*fbar): stays 0 wherever fbar >= 0, stored only on change
+        const float cn = fminf(fmaf(smu, fcs[e], cs[e]), 0.f);
+        if (cn != cs[e]) c[t + e] = cn;
+      }
+      *reinterpret_cast<float4*>(p + t) = make_float4(np[0], np[1], np[2], np[3]);
+      *reinterpret_cast<float4*>(q + t) = make_float4(nq[0], nq[1], nq[2], nq[3]);
+      *reinterpret_cast<float4*>(s + t) = make_float4(ns[0], ns[1], ns[2], ns[3]);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const unsigned int k0 = __float_as_uint(np[e]) & 0x7FFFFFFFu;
+        const unsigned int k1 = __float_as_uint(nq[e]) & 0x7FFFFFFFu;
+        const unsigned int k2 = __float_as_uint(ns[e]) & 0x7FFFFFFFu;
+        kmax[0] = max(kmax[0], k0);
+        kmax[1] = max(kmax[1], k1);
+        kmax[2] = max(kmax[2], k2);
+        hist_add(hs[0], kL1B1, (int)(k0 >> kL1S1), k0, true);
+        hist_add(hs[1], kL1B1, (int)(k1 >> kL1S1), k1, true);
+        hist_add(hs[2], kL1B1, (int)(k2 >> kL1S1), k2, true);
+      }
+      fc = fn;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    hist_flush(hs[a], kL1B1, chans[a].cnt1, chans[a].sum1);
+    unsigned int km = kmax[a];
+    for (int o = 16; o > 0; o >>= 1) km = max(km, __shfl_xor_sync(0xffffffffu, km, o));
+    if ((ltid() & 31) == 0 && km) atomicMax(&chans[a].maxkey, km);
+  }
+}
+
 __device__ __forceinline__ float clipf(float x, float m) { return copysignf(fminf(fabsf(x), m), x); }
 
 // ---- fused PDHG primal step (DTVCP.py:44-54) ----------------------------------------------------
@@ -1002,7 +1130,29 @@ int dtv_pdhg_dual(const void* fbar, float* p, float* q, float* s, float* c, cons
                                           (tiles + per_block - 1) / per_block);
   l1_reset_kernel<<<3, kL1ResetThreads, 0, st>>>(ch, 3, nullptr, t, sg * prm->v[0], sg * prm->v[1],
                                     sg * prm->v[2]); note_launch();
-  if (prm->f_dtype == DTV_F32) {
+  // four x per thread where rows (and, with the D_y wrap, the row count) are
+  // multiples of 4 and the arrays allow 16-byte (8-byte for 16-bit fbar) access
+  const int fb_align = prm->f_dtype == DTV_F32 ? 16 : 8;
+  const bool x4 = d.X % 4 == 0 && (!d.quirk || d.Y % 4 == 0) &&
+                  ((uintptr_t)p | (uintptr_t)q | (uintptr_t)s | (uintptr_t)c) % 16 == 0 &&
+                  (uintptr_t)fbar % fb_align == 0;
+  if (x4) {
+    const int64_t t4 = (int64_t)((d.X + kX4TX - 1) / kX4TX) * ((d.Y + kTY - 1) / kTY) *
+                       ((d.Z + kX4ZS - 1) / kX4ZS) * batch;
+    const int64_t per4 = kHistBlockElems / (kX4TX * kTY * kX4ZS);
+    const int g4 = (int)std::max<int64_t>(std::min<int64_t>(t4, 148LL * 4), (t4 + per4 - 1) / per4);
+    const float b0 = prm->v[0] * sg, b1 = prm->v[1] * sg, b2 = prm->v[2] * sg, sm = sg * prm->mu;
+    if (prm->f_dtype == DTV_F32)
+      pdhg_dual_x4_kernel<float><<<g4, kBlock3, 0, st>>>((const float*)fbar, p, q, s, c, d, b0,
+                                                          b1, b2, sm, ch, (int)t4);
+    else if (prm->f_dtype == DTV_F16)
+      pdhg_dual_x4_kernel<__half><<<g4, kBlock3, 0, st>>>((const __half*)fbar, p, q, s, c, d, b0,
+                                                           b1, b2, sm, ch, (int)t4);
+    else
+      pdhg_dual_x4_kernel<__nv_bfloat16><<<g4, kBlock3, 0, st>>>(
+          (const __nv_bfloat16*)fbar, p, q, s, c, d, b0, b1, b2, sm, ch, (int)t4);
+    note_launch();
+  } else if (prm->f_dtype == DTV_F32) {
     pdhg_dual_kernel<float><<<grid, kBlock3, 0, st>>>(
         (const float*)fbar, p, q, s, c, dd, prm->v[0] * sg, prm->v[1] * sg, prm->v[2] * sg,
         sg * prm->mu, ch, tiles); note_launch();

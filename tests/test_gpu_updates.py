@@ -152,6 +152,50 @@ def test_pdhg_dual_workspace_of_any_contents(cuda):
             assert torch.equal(a, b)
 
 
+@pytest.mark.parametrize("fdt", [torch.float32, torch.float16])
+@pytest.mark.parametrize("quirk", [True, False])
+def test_pdhg_dual_vector_path_equals_scalar_path(cuda, fdt, quirk):
+    """Rows of a multiple of 4 voxels take the dual step four x at a time
+    (16-byte duals); an f-bar or c that is not 16-byte (8-byte) aligned sends
+    it down the one-voxel path. Both give the same bits, thresholds included."""
+    import ctypes
+    from dtvb200.geometry import _ptr, _stream
+    rng = np.random.default_rng(11)
+    vs = (24, 16, 10)
+    X, Y, Z = vs
+    n = X * Y * Z
+    fbar = rng.random(n).astype(np.float32)
+    duals = [(rng.standard_normal(n) * 0.01).astype(np.float32) for _ in range(4)]
+    duals[3] = -np.abs(duals[3])  # c <= 0
+    prm = _lib.dtv_pdhg_params()
+    prm.sigma, prm.tau, prm.mu = 0.05, 0.02, 0.7
+    prm.v[:] = (0.4, 0.3, 0.2)
+    prm.quirk = int(quirk)
+    prm.f_dtype = _lib.DTV_F32 if fdt == torch.float32 else _lib.DTV_F16
+    tt = torch.tensor([3.0, 2.0, 1.5], dtype=torch.float64, device=cuda)
+    nbytes = _lib.load().dtv_pdhg_workspace_bytes()
+    res = []
+    for off in (0, 1):  # element offset 1: f-bar and c 4-byte (2-byte) aligned
+        fb = torch.zeros(n + 4, dtype=fdt, device=cuda)[off:off + n]
+        fb.copy_(torch.from_numpy(fbar))
+        arrs = []
+        for j, d in enumerate(duals):
+            o = off if j == 3 else 0  # p, q, s stay 16-byte aligned, as required
+            a = torch.zeros(n + 4, device=cuda)[o:o + n]
+            a.copy_(torch.from_numpy(d))
+            arrs.append(a)
+        ws = torch.zeros(nbytes, dtype=torch.uint8, device=cuda)
+        _lib.call("dtv_pdhg_dual", _ptr(fb), *[_ptr(a) for a in arrs], _lib.ivec(vs), 1,
+                  ctypes.byref(prm), _ptr(tt), _ptr(ws), _stream(cuda))
+        torch.cuda.synchronize()
+        thr = [ws[k * nbytes // 3 + 44:k * nbytes // 3 + 48].cpu() for k in range(3)]
+        res.append(([a.cpu() for a in arrs], thr))
+    for a, b in zip(res[0][0], res[1][0]):
+        assert torch.equal(a, b)
+    for a, b in zip(res[0][1], res[1][1]):
+        assert torch.equal(a, b)
+
+
 def _pdhg_case(cuda, fdt=torch.float32, quirk=True):
     rng = np.random.default_rng(5)
     vs = (20, 16, 12)
