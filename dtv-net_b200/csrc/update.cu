@@ -826,9 +826,113 @@ __global__ void __launch_bounds__(256) pdhg_primal_kernel(float* __restrict__ f,
     const int64_t t = cl.base + i;
     const float reg = fmaf(v0, dx, fmaf(v1, dy, fmaf(v2, dz, mu * c[t])));
     const float fo = f[t];
-    const float fn = fo - recon[t] - tau * reg;
-    store_from_float(fbar, t, 2.f * fn - fo);
+    // explicit FMAs: every instance of the step rounds the same way
+    const float fn = fmaf(-tau, reg, fo - recon[t]);
+    store_from_float(fbar, t, fmaf(2.f, fn, -fo));
     f[t] = fn;
+  }
+}
+
+// Four floats as a 16-bit or 32-bit vector store (16-byte aligned for float,
+// 8-byte for the 16-bit types).
+__device__ __forceinline__ void store4_from_float(float* p, int64_t i, float4 v) {
+  *reinterpret_cast<float4*>(p + i) = v;
+}
+__device__ __forceinline__ void store4_from_float(__half* p, int64_t i, float4 v) {
+  const __half2 a = __floats2half2_rn(v.x, v.y), b = __floats2half2_rn(v.z, v.w);
+  uint2 w;
+  w.x = *reinterpret_cast<const unsigned int*>(&a);
+  w.y = *reinterpret_cast<const unsigned int*>(&b);
+  *reinterpret_cast<uint2*>(p + i) = w;
+}
+__device__ __forceinline__ void store4_from_float(__nv_bfloat16* p, int64_t i, float4 v) {
+  const __nv_bfloat162 a = __floats2bfloat162_rn(v.x, v.y), b = __floats2bfloat162_rn(v.z, v.w);
+  uint2 w;
+  w.x = *reinterpret_cast<const unsigned int*>(&a);
+  w.y = *reinterpret_cast<const unsigned int*>(&b);
+  *reinterpret_cast<uint2*>(p + i) = w;
+}
+
+// The primal step with four consecutive x per thread (the conditions of
+// pdhg_dual_x4_kernel): 16-byte loads of f, the backprojection, the duals
+// and c; the x-neighbour of the first voxel comes from one scalar load, the
+// others from the thread's own vector. Same arithmetic per voxel as
+// pdhg_primal_kernel.
+template <class T>
+__global__ void __launch_bounds__(256) pdhg_primal_x4_kernel(float* __restrict__ f,
+                                                             T* __restrict__ fbar,
+                                                             const float* __restrict__ recon,
+                                                             float* p, float* q, float* s,
+                                                             const float* __restrict__ c, Dims d,
+                                                             float tau, float mu, float v0,
+                                                             float v1, float v2,
+                                                             const L1Chan* chans) {
+  const int x0 = (blockIdx.x * kTX + (int)threadIdx.x) * 4;
+  const int y = blockIdx.y * kTY + (int)threadIdx.y;
+  const int zslabs = (d.Z + d.zs - 1) / d.zs;
+  const int z0 = (int)(blockIdx.z % zslabs) * d.zs;
+  const int nz = min(d.zs, d.Z - z0);
+  if (x0 >= d.X || y >= d.Y) return;
+  const int64_t base = (int64_t)(blockIdx.z / zslabs) * d.N;
+  const float m0 = chans[0].thresh, m1 = chans[1].thresh, m2 = chans[2].thresh;
+  const int64_t plane = (int64_t)d.X * d.Y;
+  const int64_t oy = axis_off(d, 1);
+  float* pb = p + base;
+  float* qb = q + base;
+  float* sb = s + base;
+  int64_t i = ((int64_t)z0 * d.Y + y) * d.X + x0;
+  float sprev[4] = {0.f, 0.f, 0.f, 0.f};  // clipped s(i - XY), carried along z
+  if (z0 >= 1) {
+    const float4 sv = *reinterpret_cast<const float4*>(sb + i - plane);
+    sprev[0] = clipf(sv.x, m2); sprev[1] = clipf(sv.y, m2);
+    sprev[2] = clipf(sv.z, m2); sprev[3] = clipf(sv.w, m2);
+  }
+  for (int k = 0; k < nz; ++k, i += plane) {
+    const float4 P = *reinterpret_cast<const float4*>(pb + i);
+    const float4 Q = *reinterpret_cast<const float4*>(qb + i);
+    const float4 S = *reinterpret_cast<const float4*>(sb + i);
+    const int64_t t = base + i;
+    const float4 Cv = __ldg(reinterpret_cast<const float4*>(c + t));
+    const float4 Fv = *reinterpret_cast<const float4*>(f + t);
+    const float4 Rv = __ldg(reinterpret_cast<const float4*>(recon + t));
+    const float pr[4] = {P.x, P.y, P.z, P.w}, qr[4] = {Q.x, Q.y, Q.z, Q.w};
+    const float sr[4] = {S.x, S.y, S.z, S.w}, cs[4] = {Cv.x, Cv.y, Cv.z, Cv.w};
+    const float fo[4] = {Fv.x, Fv.y, Fv.z, Fv.w}, rc[4] = {Rv.x, Rv.y, Rv.z, Rv.w};
+    float ps[4], qs[4], ss[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      ps[e] = clipf(pr[e], m0);
+      qs[e] = clipf(qr[e], m1);
+      ss[e] = clipf(sr[e], m2);
+    }
+    const float pl = x0 >= 1 ? clipf(pb[i - 1], m0) : 0.f;  // the first voxel's x-neighbour
+    const bool yv = d.quirk ? (i >= d.Y) : (y >= 1);        // shared by the four (aligned)
+    float qn[4] = {0.f, 0.f, 0.f, 0.f};
+    if (yv) {
+      const float4 Qn = *reinterpret_cast<const float4*>(qb + i - oy);
+      qn[0] = clipf(Qn.x, m1); qn[1] = clipf(Qn.y, m1);
+      qn[2] = clipf(Qn.z, m1); qn[3] = clipf(Qn.w, m1);
+    }
+    const bool zv = z0 + k >= 1;
+    float fn[4], fb[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      float dx = -ps[e], dy = -qs[e], dz = -ss[e];
+      if (e > 0) dx += ps[e - 1];
+      else if (x0 >= 1) dx += pl;
+      if (yv) dy += qn[e];
+      if (zv) dz += sprev[e];
+      // only clipped duals change; the others keep their bytes without a store
+      if (ps[e] != pr[e]) pb[i + e] = ps[e];
+      if (qs[e] != qr[e]) qb[i + e] = qs[e];
+      if (ss[e] != sr[e]) sb[i + e] = ss[e];
+      sprev[e] = ss[e];
+      const float reg = fmaf(v0, dx, fmaf(v1, dy, fmaf(v2, dz, mu * cs[e])));
+      fn[e] = fmaf(-tau, reg, fo[e] - rc[e]);
+      fb[e] = fmaf(2.f, fn[e], -fo[e]);
+    }
+    store4_from_float(fbar, t, make_float4(fb[0], fb[1], fb[2], fb[3]));
+    *reinterpret_cast<float4*>(f + t) = make_float4(fn[0], fn[1], fn[2], fn[3]);
   }
 }
 
@@ -1198,7 +1302,35 @@ int dtv_pdhg_primal(float* f, void* fbar, const float* recon, float* p, float* q
   if (rc) return rc;
   Dims d = make_dims(size, prm->quirk, batch);
   const L1Chan* ch = reinterpret_cast<const L1Chan*>(ws);
-  if (prm->f_dtype == DTV_F32) {
+  // four x per thread under the conditions of the dual step's vector path
+  const int fb_align = prm->f_dtype == DTV_F32 ? 16 : 8;
+  const bool x4 = d.X % 4 == 0 && (!d.quirk || d.Y % 4 == 0) &&
+                  ((uintptr_t)f | (uintptr_t)recon | (uintptr_t)p | (uintptr_t)q | (uintptr_t)s |
+                   (uintptr_t)c) % 16 == 0 &&
+                  (uintptr_t)fbar % fb_align == 0;
+  if (x4) {
+    // a quarter of the x blocks: halve the slices per thread while the grid
+    // has fewer than four blocks per SM
+    Dims d4 = d;
+    const int64_t cols = (int64_t)((d.X / 4 + kTX - 1) / kTX) * ((d.Y + kTY - 1) / kTY);
+    while (d4.zs > 1 && cols * ((d.Z + d4.zs - 1) / d4.zs) * batch < kWantBlocks) d4.zs /= 2;
+    const dim3 g4((d.X / 4 + kTX - 1) / kTX, (d.Y + kTY - 1) / kTY,
+                  ((d.Z + d4.zs - 1) / d4.zs) * batch);
+    cudaStream_t st = as_stream(stream);
+    if (prm->f_dtype == DTV_F32)
+      pdhg_primal_x4_kernel<float><<<g4, kBlock3, 0, st>>>(f, (float*)fbar, recon, p, q, s, c,
+                                                           d4, prm->tau, prm->mu, prm->v[0],
+                                                           prm->v[1], prm->v[2], ch);
+    else if (prm->f_dtype == DTV_F16)
+      pdhg_primal_x4_kernel<__half><<<g4, kBlock3, 0, st>>>(f, (__half*)fbar, recon, p, q, s, c,
+                                                            d4, prm->tau, prm->mu, prm->v[0],
+                                                            prm->v[1], prm->v[2], ch);
+    else
+      pdhg_primal_x4_kernel<__nv_bfloat16><<<g4, kBlock3, 0, st>>>(
+          f, (__nv_bfloat16*)fbar, recon, p, q, s, c, d4, prm->tau, prm->mu, prm->v[0],
+          prm->v[1], prm->v[2], ch);
+    note_launch();
+  } else if (prm->f_dtype == DTV_F32) {
     pdhg_primal_kernel<float><<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(
         f, (float*)fbar, recon, p, q, s, c, d, prm->tau, prm->mu, prm->v[0], prm->v[1],
         prm->v[2], ch); note_launch();

@@ -196,6 +196,51 @@ def test_pdhg_dual_vector_path_equals_scalar_path(cuda, fdt, quirk):
         assert torch.equal(a, b)
 
 
+@pytest.mark.parametrize("fdt", [torch.float32, torch.float16])
+@pytest.mark.parametrize("quirk", [True, False])
+def test_pdhg_primal_vector_path_equals_scalar_path(cuda, fdt, quirk):
+    """The primal step four x at a time (16-byte loads) against the one-voxel
+    path (taken when f-bar or c is not aligned): the same bits of f, f-bar
+    and the clipped duals."""
+    import ctypes
+    from dtvb200.geometry import _ptr, _stream
+    rng = np.random.default_rng(12)
+    vs = (24, 16, 10)
+    X, Y, Z = vs
+    n = X * Y * Z
+    host = {k: rng.random(n).astype(np.float32) for k in ("f", "fbar")}
+    host["recon"] = (rng.standard_normal(n) * 0.01).astype(np.float32)
+    for k in ("p", "q", "s"):
+        host[k] = (rng.standard_normal(n) * 0.05).astype(np.float32)
+    host["c"] = -np.abs(rng.standard_normal(n) * 0.01).astype(np.float32)
+    prm = _lib.dtv_pdhg_params()
+    prm.sigma, prm.tau, prm.mu = 0.05, 0.02, 0.7
+    prm.v[:] = (0.4, 0.3, 0.2)
+    prm.quirk = int(quirk)
+    prm.f_dtype = _lib.DTV_F32 if fdt == torch.float32 else _lib.DTV_F16
+    nbytes = _lib.load().dtv_pdhg_workspace_bytes()
+    ws = torch.zeros(nbytes, dtype=torch.uint8, device=cuda)
+    for k, thr in enumerate((0.03, 0.02, 0.04)):  # the three channels' thresholds
+        ws[k * nbytes // 3 + 44:k * nbytes // 3 + 48] = torch.from_numpy(
+            np.array([thr], np.float32).view(np.uint8)).to(cuda)
+    res = []
+    for off in (0, 1):
+        T = {}
+        for k, a in host.items():
+            o = off if k in ("fbar", "c") else 0
+            dt = fdt if k == "fbar" else torch.float32
+            t = torch.zeros(n + 4, dtype=dt, device=cuda)[o:o + n]
+            t.copy_(torch.from_numpy(a))
+            T[k] = t
+        _lib.call("dtv_pdhg_primal", _ptr(T["f"]), _ptr(T["fbar"]), _ptr(T["recon"]),
+                  _ptr(T["p"]), _ptr(T["q"]), _ptr(T["s"]), _ptr(T["c"]), _lib.ivec(vs), 1,
+                  ctypes.byref(prm), _ptr(ws), _stream(cuda))
+        torch.cuda.synchronize()
+        res.append({k: T[k].cpu() for k in ("f", "fbar", "p", "q", "s")})
+    for k in res[0]:
+        assert torch.equal(res[0][k], res[1][k]), k
+
+
 def _pdhg_case(cuda, fdt=torch.float32, quirk=True):
     rng = np.random.default_rng(5)
     vs = (20, 16, 12)
