@@ -229,19 +229,15 @@ __global__ void __launch_bounds__(256) diff_kernel(const float* __restrict__ f, 
 }
 
 template <class T>
-// A grid of a few blocks per SM walks the (x, y, z-slab) tiles, so each
-// block adds its three sums to the device totals once (one FP64 atomic per
-// block and channel, instead of one per tile: those contended on three
-// addresses and took most of the time).
 __global__ void __launch_bounds__(256) diff_abs_sums_kernel(const T* __restrict__ f, Dims d,
-                                                            double* __restrict__ sums,
-                                                            int64_t n_tiles) {
+                                                            double* __restrict__ sums) {
+  const Col c = col3(d);
   double acc[3] = {0.0, 0.0, 0.0};
-  for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
-    const Col c = col3_tile(d, tile);
-    if (!c.in) continue;
+  if (c.in) {
     const T* fb = f + c.base;
     float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+    // unrolled: the slices' loads are independent and can all be in flight
+#pragma unroll 4
     for (int k = 0; k < c.nz; ++k) {
       const int z = c.z0 + k;
       const int64_t i = ((int64_t)z * d.Y + c.y) * d.X + c.x;
@@ -249,7 +245,7 @@ __global__ void __launch_bounds__(256) diff_abs_sums_kernel(const T* __restrict_
       s1 += fabsf(dfwd(fb, d, 1, i, c.x, c.y, z));
       s2 += fabsf(dfwd(fb, d, 2, i, c.x, c.y, z));
     }
-    acc[0] += s0; acc[1] += s1; acc[2] += s2;
+    acc[0] = s0; acc[1] = s1; acc[2] = s2;
   }
   block_sums_atomic<3>(acc, sums);
 }
@@ -1179,15 +1175,12 @@ int dtv_diff_abs_sums(const void* f, int32_t dt, const int32_t size[3], int32_t 
   int rc = check_dims(size, batch);
   if (rc) return rc;
   Dims d = make_dims(size, quirk, batch);
-  const dim3 g = grid3(d, batch);
-  const int64_t tiles = (int64_t)g.x * g.y * g.z;
-  const int blocks = (int)std::min<int64_t>(tiles, 148LL * 8);
   if (dt == DTV_F32) {
-    diff_abs_sums_kernel<float><<<blocks, kBlock3, 0, as_stream(stream)>>>(
-        (const float*)f, d, sums, tiles); note_launch();
+    diff_abs_sums_kernel<float><<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(
+        (const float*)f, d, sums); note_launch();
   } else {
-    diff_abs_sums_kernel<__half><<<blocks, kBlock3, 0, as_stream(stream)>>>(
-        (const __half*)f, d, sums, tiles); note_launch();
+    diff_abs_sums_kernel<__half><<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(
+        (const __half*)f, d, sums); note_launch();
   }
   DTV_LAUNCH_CHECK();
   return DTV_OK;
