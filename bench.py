@@ -36,9 +36,9 @@ CFG = dict(nx=256, ny=256, nz=256, voxel=1.0, nu=384, nv=384, pitch=1.2, n_views
 
 # DRAM traffic of one forward-projector launch on this workload
 # (dram__bytes_read.sum + dram__bytes_write.sum) and the texture-pipe
-# utilisation of that launch, from the ncu capture summarised in
-# profiles/fp_pair_kernel_sparse_view_dtv.md (`python bench.py --profile 12`).
-# They describe the kernel as captured there, not this run.
+# utilisation of that launch, from one `ncu --set full` capture of the 13th
+# forward projection of `python bench.py --profile 12`. They describe the
+# kernel as captured then, not this run; "source" names the summary.
 FP_NCU = {"pairs": {"traffic": 142.743040e6 + 28.150784e6, "tex_pipe_pct": 95.4,
                     "source": "profiles/fp_pair_kernel_sparse_view_dtv.md"}}
 

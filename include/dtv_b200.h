@@ -43,7 +43,7 @@ extern "C" {
 #define DTV_ERR_INVALID 1     /* bad argument (null, size, dtype, ...)     */
 #define DTV_ERR_CUDA 2        /* a CUDA runtime call failed                */
 #define DTV_ERR_ALLOC 3       /* device allocation failed                  */
-#define DTV_ERR_UNSUPPORTED 4 /* valid but not supported by this build     */
+#define DTV_ERR_UNSUPPORTED 4 /* valid but not supported by the library   */
 
 /* ---- storage types ------------------------------------------------------ */
 #define DTV_F32 0
