@@ -52,12 +52,12 @@ def test_forward_refresh_equals_separate_passes(cuda, dtype, batch):
     assert abs(s.item() - s_ref.item()) <= 1e-12 * s_ref.item()
 
 
-@pytest.mark.parametrize("views", [20, 700])  # 700: two view chunks of the launch parameters
-def test_backward_refresh_equals_separate_passes(cuda, views):
+@pytest.mark.parametrize("views,batch", [(20, 1), (20, 2), (700, 1)])  # 700: two view chunks
+def test_backward_refresh_equals_separate_passes(cuda, views, batch):
     n = 40 if views == 20 else 16
-    fast, exact = plans(cuda, n=n, views=views)
-    sino = torch.rand(fast.sino_shape(1), device=cuda)
-    out = torch.full(fast.vol_shape(1), float("nan"), device=cuda)
+    fast, exact = plans(cuda, n=n, views=views, batch=batch)
+    sino = torch.rand(fast.sino_shape(batch), device=cuda)
+    out = torch.full(fast.vol_shape(batch), float("nan"), device=cuda)
     e_b = torch.full_like(out, float("nan"))
     dtvb200.backward_refresh(fast, exact, sino, out, e_b)
     be = exact.backward(sino)
