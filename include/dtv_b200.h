@@ -266,7 +266,8 @@ DTV_API int dtv_forward(dtv_plan* plan, const void* vol, int32_t vol_dtype, int3
 DTV_API int dtv_backward(dtv_plan* plan, const float* sino, int32_t batch, float* out, int32_t accumulate,
                  void* stream);
 /* out = base + BP(sino), same backprojector as dtv_backward; base may equal
- * out (then it is dtv_backward with accumulate != 0). No reference
+ * out (then it is dtv_backward with accumulate != 0), or else must not
+ * overlap it. No reference
  * counterpart: DTVCP's corrected iterations add the stored backprojector
  * correction this way without copying it into out first. */
 DTV_API int dtv_backward_onto(dtv_plan* plan, const float* sino, int32_t batch, const float* base,
