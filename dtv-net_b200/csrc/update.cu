@@ -1315,7 +1315,9 @@ int dtv_pdhg_primal(float* f, void* fbar, const float* recon, float* p, float* q
     // has fewer than four blocks per SM
     Dims d4 = d;
     const int64_t cols = (int64_t)((d.X / 4 + kTX - 1) / kTX) * ((d.Y + kTY - 1) / kTY);
-    while (d4.zs > 1 && cols * ((d.Z + d4.zs - 1) / d4.zs) * batch < kWantBlocks) d4.zs /= 2;
+    while (d4.zs > 1 && cols * ((d.Z + d4.zs - 1) / d4.zs) * batch < kWantBlocks &&
+           (int64_t)((d.Z + d4.zs / 2 - 1) / (d4.zs / 2)) * batch <= 65535)
+      d4.zs /= 2;
     const dim3 g4((d.X / 4 + kTX - 1) / kTX, (d.Y + kTY - 1) / kTY,
                   ((d.Z + d4.zs - 1) / d4.zs) * batch);
     cudaStream_t st = as_stream(stream);
