@@ -24,6 +24,7 @@ struct BPParams {
   float scale;
   int64_t sino_pad_elems;  // one padded view
   int warp;                // columns of a warp and a quad (DTV_TUNE_BP_WARP)
+  int vsplit;              // 2: two halves of a block sum the two halves of the views
 };
 
 constexpr int kBPTile = 16;  // columns per block edge
@@ -105,7 +106,11 @@ struct TableMaps {
 };
 
 // One block's columns: tile `tile` of 16x16 (x, y) columns, z-chunk `zc` of ZC
-// voxels, views n0 .. n0 + n_chunk - 1.
+// voxels, views n0 .. n0 + n_chunk - 1. With bp.vsplit == 2 (volumes too small
+// to fill the GPU otherwise) the tile is 16x8 columns and the block's two
+// halves take the first and the second half of the views; the second half's
+// sums are added to the first's through shared memory, in that order, so the
+// result is deterministic.
 template <int kSrc, bool kZAff, int ZC, class Maps>
 __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps, int n0, int n_chunk,
                                            const float* __restrict__ spad, cudaTextureObject_t tex,
@@ -115,8 +120,13 @@ __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps,
   // 4 x 8 columns (the narrower, the fewer detector rows' cache sectors one
   // fetch instruction touches when a voxel spans several pixels)
   const int t = (int)threadIdx.x;
+  const bool split = bp.vsplit == 2;
+  const int half = split ? t >> 7 : 0;
   int li, lj;
-  if (bp.warp >= 3) {
+  if (split) {
+    li = t & 15;
+    lj = (t & 127) >> 4;
+  } else if (bp.warp >= 3) {
     // quads (4 consecutive lanes) of 2 x 2 columns; a warp of 8 quads covers
     // 8 x 4 (warp 3) or 4 x 8 (warp 4) columns
     const int q = (t >> 2) & 7, qi = t & 1, qj = (t >> 1) & 1, w = t >> 5;
@@ -138,9 +148,14 @@ __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps,
     lj = t >> 4;
   }
   const int i = (tile % tiles_x) * kBPTile + li;
-  const int j = (tile / tiles_x) * kBPTile + lj;
+  const int j = (tile / tiles_x) * (split ? kBPTile / 2 : kBPTile) + lj;
   const int k0 = zc * ZC;
-  if (i >= bp.nx || j >= bp.ny) return;
+  const bool valid = i < bp.nx && j < bp.ny;
+  if (!valid && !split) return;  // the split halves meet at a barrier below
+  // this thread's views: all of the chunk, or one half of it
+  const int hv = (n_chunk + 1) / 2;
+  const int jn0 = split ? half * hv : 0;
+  const int jn1 = !valid ? jn0 : (split && half == 0 ? hv : n_chunk);
   constexpr bool kBoth = kSrc == kSrcBoth;
   float acc[ZC], act[kBoth ? ZC : 1];
 #pragma unroll
@@ -150,7 +165,7 @@ __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps,
   const float fi = (float)i, fj = (float)j;
   const int pu = bp.nu + 2 * kPad;
   const float mu = (float)bp.nu, mv = (float)bp.nv;
-  for (int jn = 0; jn < n_chunk; ++jn) {
+  for (int jn = jn0; jn < jn1; ++jn) {
     const int n = n0 + jn;
     const float* w = maps.row(jn);
     const float m0 = w[0], m1 = w[1], m2 = w[2], m3 = w[3];
@@ -210,6 +225,26 @@ __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps,
         acc[z] = fmaf(val, wgt, acc[z]);
         if constexpr (kBoth) act[z] = fmaf(tex2DLayered<float>(tex, tu, tv, n), wgt, act[z]);
       }
+    }
+  }
+  if (split) {
+    // the second half hands its sums to the first: acc = first + second
+    // (dynamic shared memory, given only to split launches)
+    extern __shared__ float red[];
+    const int lt = t & 127;
+    if (half == 1) {
+#pragma unroll
+      for (int z = 0; z < ZC; ++z) {
+        red[z * 128 + lt] = acc[z];
+        if constexpr (kBoth) red[(ZC + z) * 128 + lt] = act[z];
+      }
+    }
+    __syncthreads();
+    if (half == 1 || !valid) return;
+#pragma unroll
+    for (int z = 0; z < ZC; ++z) {
+      acc[z] = acc[z] + red[z * 128 + lt];
+      if constexpr (kBoth) act[z] = act[z] + red[(ZC + z) * 128 + lt];
     }
   }
   const int64_t plane = (int64_t)bp.nx * bp.ny;
@@ -283,12 +318,15 @@ template <int kSrc, bool kZAff>
 static void launch_bp_zc(int zc, dim3 grid, cudaStream_t st, const BPParams& bp,
                          const BPMaps& maps, int n0, int cnt, const float* sp,
                          cudaTextureObject_t tx, const BPOut& dst) {
+  // split launches: the second half's sums of each voxel in shared memory
+  const size_t sm = bp.vsplit == 2 ? (size_t)(kSrc == kSrcBoth ? 2 : 1) * zc * 128 * sizeof(float)
+                                   : 0;
   if (zc == 8)
-    bp_kernel<kSrc, kZAff, 8><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, dst);
+    bp_kernel<kSrc, kZAff, 8><<<grid, kBPThreads, sm, st>>>(bp, maps, n0, cnt, sp, tx, dst);
   else if (zc == 4)
-    bp_kernel<kSrc, kZAff, 4><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, dst);
+    bp_kernel<kSrc, kZAff, 4><<<grid, kBPThreads, sm, st>>>(bp, maps, n0, cnt, sp, tx, dst);
   else
-    bp_kernel<kSrc, kZAff, 2><<<grid, kBPThreads, 0, st>>>(bp, maps, n0, cnt, sp, tx, dst);
+    bp_kernel<kSrc, kZAff, 2><<<grid, kBPThreads, sm, st>>>(bp, maps, n0, cnt, sp, tx, dst);
 }
 
 template <int kSrc>
@@ -310,6 +348,20 @@ static void launch_bp(int src, bool zaff, int zc, dim3 grid, cudaStream_t st, co
   }
 }
 
+// Column tiles of 16 x 16, or of 16 x 8 where the plan splits its views.
+static int bp_tiles(const GeomParams& gp, int vsplit) {
+  const int th = vsplit == 2 ? kBPTile / 2 : kBPTile;
+  return ((gp.nx + kBPTile - 1) / kBPTile) * ((gp.ny + th - 1) / th);
+}
+
+// A volume whose 16 x 16 column tiles cannot give four blocks per SM even with
+// two slices per thread splits its views between two halves of each block
+// (twice the blocks, half the views each). A property of the plan's geometry
+// alone, so every launch of the plan sums its views in the same order.
+static int bp_vsplit(const GeomParams& gp) {
+  return gp.n_views >= 2 && (int64_t)bp_tiles(gp, 1) * ((gp.nz + 1) / 2) < kBPWantBlocks ? 2 : 1;
+}
+
 static BPParams plan_bp_params(const Plan* p) {
   const GeomParams& gp = p->gp;
   BPParams bp;
@@ -320,6 +372,7 @@ static BPParams plan_bp_params(const Plan* p) {
   bp.scale = (float)gp.bp_scale;
   bp.sino_pad_elems = (int64_t)(gp.nu + 2 * kPad) * (gp.nv + 2 * kPad);
   bp.warp = p->bp_warp;
+  bp.vsplit = bp_vsplit(gp);
   return bp;
 }
 
@@ -351,7 +404,7 @@ static int stage_sino(Plan* p, const float* sino, cudaStream_t st) {
 }
 
 static dim3 bp_grid(const GeomParams& gp, int* zc_out) {
-  const int tiles = ((gp.nx + kBPTile - 1) / kBPTile) * ((gp.ny + kBPTile - 1) / kBPTile);
+  const int tiles = bp_tiles(gp, bp_vsplit(gp));
   const int zc = bp_zc([&](int c) { return (int64_t)tiles * ((gp.nz + c - 1) / c); });
   *zc_out = zc;
   return dim3(tiles, (gp.nz + zc - 1) / zc);
@@ -499,8 +552,7 @@ int backward_many_impl(Plan* const* plans, const float* const* sinos, float* con
       int64_t b = 0;
       for (int k = 0; k < cnt; ++k) {
         const GeomParams& gp = plans[c0 + k]->gp;
-        b += (int64_t)((gp.nx + kBPTile - 1) / kBPTile) * ((gp.ny + kBPTile - 1) / kBPTile) *
-             ((gp.nz + c - 1) / c);
+        b += (int64_t)bp_tiles(gp, bp_vsplit(gp)) * ((gp.nz + c - 1) / c);
       }
       return b;
     });
@@ -522,7 +574,7 @@ int backward_many_impl(Plan* const* plans, const float* const* sinos, float* con
       it.views = p->d_bpv;
       it.tex = p->sino_tex[0];
       it.out = outs[c0 + k];
-      it.tiles = ((gp.nx + kBPTile - 1) / kBPTile) * ((gp.ny + kBPTile - 1) / kBPTile);
+      it.tiles = bp_tiles(gp, it.bp.vsplit);
       it.block0 = (int)blocks;
       it.zaffine = p->bp_zaffine;
       it.map0 = -1;
@@ -535,9 +587,12 @@ int backward_many_impl(Plan* const* plans, const float* const* sinos, float* con
     }
     DTV_CHECK(blocks < 2147483647LL, "too many blocks for one launch");
     m.count = cnt;
-    if (zc == 8) bp_many_kernel<8><<<(unsigned)blocks, kBPThreads, 0, st>>>(m, accumulate);
-    else if (zc == 4) bp_many_kernel<4><<<(unsigned)blocks, kBPThreads, 0, st>>>(m, accumulate);
-    else bp_many_kernel<2><<<(unsigned)blocks, kBPThreads, 0, st>>>(m, accumulate);
+    bool any_split = false;
+    for (int k = 0; k < cnt; ++k) any_split |= m.it[k].bp.vsplit == 2;
+    const size_t sm = any_split ? (size_t)zc * 128 * sizeof(float) : 0;
+    if (zc == 8) bp_many_kernel<8><<<(unsigned)blocks, kBPThreads, sm, st>>>(m, accumulate);
+    else if (zc == 4) bp_many_kernel<4><<<(unsigned)blocks, kBPThreads, sm, st>>>(m, accumulate);
+    else bp_many_kernel<2><<<(unsigned)blocks, kBPThreads, sm, st>>>(m, accumulate);
     note_launch();
     DTV_LAUNCH_CHECK();
     c0 += cnt;
