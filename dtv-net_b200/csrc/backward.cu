@@ -11,6 +11,7 @@
 // gives the detector coordinates with one reciprocal per voxel-view.
 #include <algorithm>
 #include <type_traits>
+#include <vector>
 #include <string.h>
 
 #include "common.cuh"
@@ -111,7 +112,7 @@ struct TableMaps {
 // halves take the first and the second half of the views; the second half's
 // sums are added to the first's through shared memory, in that order, so the
 // result is deterministic.
-template <int kSrc, bool kZAff, int ZC, class Maps>
+template <int kSrc, bool kZAff, int ZC, bool kSplit, class Maps>
 __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps, int n0, int n_chunk,
                                            const float* __restrict__ spad, cudaTextureObject_t tex,
                                            const BPOut& dst, int tile, int zc) {
@@ -120,10 +121,10 @@ __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps,
   // 4 x 8 columns (the narrower, the fewer detector rows' cache sectors one
   // fetch instruction touches when a voxel spans several pixels)
   const int t = (int)threadIdx.x;
-  const bool split = bp.vsplit == 2;
+  constexpr bool split = kSplit;  // bp.vsplit == 2, chosen by the launch
   const int half = split ? t >> 7 : 0;
   int li, lj;
-  if (split) {
+  if constexpr (split) {
     li = t & 15;
     lj = (t & 127) >> 4;
   } else if (bp.warp >= 3) {
@@ -227,7 +228,7 @@ __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps,
       }
     }
   }
-  if (split) {
+  if constexpr (split) {
     // the second half hands its sums to the first: acc = first + second
     // (dynamic shared memory, given only to split launches)
     extern __shared__ float red[];
@@ -263,13 +264,13 @@ __device__ __forceinline__ void bp_columns(const BPParams& bp, const Maps& maps,
   }
 }
 
-template <int kSrc, bool kZAff, int ZC>
+template <int kSrc, bool kZAff, int ZC, bool kSplit>
 __global__ void __launch_bounds__(kBPThreads) bp_kernel(BPParams bp, const __grid_constant__ BPMaps maps,
                                                         int n0, int n_chunk,
                                                         const float* __restrict__ spad,
                                                         cudaTextureObject_t tex, BPOut dst) {
-  bp_columns<kSrc, kZAff, ZC>(bp, ParamMaps{&maps}, n0, n_chunk, spad, tex, dst,
-                              (int)blockIdx.x, (int)blockIdx.y);
+  bp_columns<kSrc, kZAff, ZC, kSplit>(bp, ParamMaps{&maps}, n0, n_chunk, spad, tex, dst,
+                                      (int)blockIdx.x, (int)blockIdx.y);
 }
 
 // Records of the exact backprojector: record (U, V) of view n from the four
@@ -314,19 +315,28 @@ static int bp_zc(BlocksFor blocks_for) {
   return 2;
 }
 
+template <int kSrc, bool kZAff, bool kSplit>
+static void launch_bp_split(int zc, dim3 grid, cudaStream_t st, const BPParams& bp,
+                            const BPMaps& maps, int n0, int cnt, const float* sp,
+                            cudaTextureObject_t tx, const BPOut& dst) {
+  // split launches: the second half's sums of each voxel in shared memory
+  const size_t sm = kSplit ? (size_t)(kSrc == kSrcBoth ? 2 : 1) * zc * 128 * sizeof(float) : 0;
+  if (zc == 8)
+    bp_kernel<kSrc, kZAff, 8, kSplit><<<grid, kBPThreads, sm, st>>>(bp, maps, n0, cnt, sp, tx, dst);
+  else if (zc == 4)
+    bp_kernel<kSrc, kZAff, 4, kSplit><<<grid, kBPThreads, sm, st>>>(bp, maps, n0, cnt, sp, tx, dst);
+  else
+    bp_kernel<kSrc, kZAff, 2, kSplit><<<grid, kBPThreads, sm, st>>>(bp, maps, n0, cnt, sp, tx, dst);
+}
+
 template <int kSrc, bool kZAff>
 static void launch_bp_zc(int zc, dim3 grid, cudaStream_t st, const BPParams& bp,
                          const BPMaps& maps, int n0, int cnt, const float* sp,
                          cudaTextureObject_t tx, const BPOut& dst) {
-  // split launches: the second half's sums of each voxel in shared memory
-  const size_t sm = bp.vsplit == 2 ? (size_t)(kSrc == kSrcBoth ? 2 : 1) * zc * 128 * sizeof(float)
-                                   : 0;
-  if (zc == 8)
-    bp_kernel<kSrc, kZAff, 8><<<grid, kBPThreads, sm, st>>>(bp, maps, n0, cnt, sp, tx, dst);
-  else if (zc == 4)
-    bp_kernel<kSrc, kZAff, 4><<<grid, kBPThreads, sm, st>>>(bp, maps, n0, cnt, sp, tx, dst);
+  if (bp.vsplit == 2)
+    launch_bp_split<kSrc, kZAff, true>(zc, grid, st, bp, maps, n0, cnt, sp, tx, dst);
   else
-    bp_kernel<kSrc, kZAff, 2><<<grid, kBPThreads, sm, st>>>(bp, maps, n0, cnt, sp, tx, dst);
+    launch_bp_split<kSrc, kZAff, false>(zc, grid, st, bp, maps, n0, cnt, sp, tx, dst);
 }
 
 template <int kSrc>
@@ -509,7 +519,8 @@ struct RowMaps {
   __device__ __forceinline__ const float* row(int jn) const { return r[jn]; }
 };
 
-template <int ZC>
+// Every item of one launch has the same bp.vsplit (kSplit).
+template <int ZC, bool kSplit>
 __global__ void __launch_bounds__(kBPThreads) bp_many_kernel(const __grid_constant__ BPMany m,
                                                              int accumulate) {
   int k = 0;
@@ -521,14 +532,14 @@ __global__ void __launch_bounds__(kBPThreads) bp_many_kernel(const __grid_consta
   if (it.map0 >= 0) {
     const RowMaps rows{m.m + it.map0};
     if (it.zaffine)
-      bp_columns<kSrcTex, true, ZC>(it.bp, rows, 0, it.bp.n_views, nullptr, it.tex, dst, tile, zc);
+      bp_columns<kSrcTex, true, ZC, kSplit>(it.bp, rows, 0, it.bp.n_views, nullptr, it.tex, dst, tile, zc);
     else
-      bp_columns<kSrcTex, false, ZC>(it.bp, rows, 0, it.bp.n_views, nullptr, it.tex, dst, tile, zc);
+      bp_columns<kSrcTex, false, ZC, kSplit>(it.bp, rows, 0, it.bp.n_views, nullptr, it.tex, dst, tile, zc);
   } else if (it.zaffine) {
-    bp_columns<kSrcTex, true, ZC>(it.bp, TableMaps{it.views}, 0, it.bp.n_views, nullptr, it.tex,
+    bp_columns<kSrcTex, true, ZC, kSplit>(it.bp, TableMaps{it.views}, 0, it.bp.n_views, nullptr, it.tex,
                                   dst, tile, zc);
   } else {
-    bp_columns<kSrcTex, false, ZC>(it.bp, TableMaps{it.views}, 0, it.bp.n_views, nullptr, it.tex,
+    bp_columns<kSrcTex, false, ZC, kSplit>(it.bp, TableMaps{it.views}, 0, it.bp.n_views, nullptr, it.tex,
                                    dst, tile, zc);
   }
 }
@@ -536,13 +547,22 @@ __global__ void __launch_bounds__(kBPThreads) bp_many_kernel(const __grid_consta
 int backward_many_impl(Plan* const* plans, const float* const* sinos, float* const* outs, int count,
                        int accumulate, cudaStream_t st) {
   BPMany m;
+  // plans that split their views run in launches of their own
+  std::vector<int> ord;
+  for (int split = 1; split <= 2; ++split)
+    for (int k = 0; k < count; ++k)
+      if (bp_vsplit(plans[k]->gp) == split) ord.push_back(k);
   int c0 = 0;
   while (c0 < count) {
-    // this launch's plans: up to kManyItems, whose maps fit the parameters
-    // (a plan with more views than fit at all takes its maps from its table)
+    // this launch's plans: up to kManyItems of one split kind, whose maps fit
+    // the parameters (a plan with more views than fit at all takes its maps
+    // from its table)
+    const int kind = bp_vsplit(plans[ord[c0]]->gp);
     int cnt = 0, rows = 0;
     while (c0 + cnt < count && cnt < kManyItems) {
-      const int nv = plans[c0 + cnt]->gp.n_views;
+      const GeomParams& g = plans[ord[c0 + cnt]]->gp;
+      if (bp_vsplit(g) != kind) break;
+      const int nv = g.n_views;
       if (nv <= kBPManyViews && rows + nv > kBPManyViews) break;
       if (nv <= kBPManyViews) rows += nv;
       ++cnt;
@@ -551,7 +571,7 @@ int backward_many_impl(Plan* const* plans, const float* const* sinos, float* con
     const int zc = bp_zc([&](int c) {
       int64_t b = 0;
       for (int k = 0; k < cnt; ++k) {
-        const GeomParams& gp = plans[c0 + k]->gp;
+        const GeomParams& gp = plans[ord[c0 + k]]->gp;
         b += (int64_t)bp_tiles(gp, bp_vsplit(gp)) * ((gp.nz + c - 1) / c);
       }
       return b;
@@ -559,11 +579,11 @@ int backward_many_impl(Plan* const* plans, const float* const* sinos, float* con
     int64_t blocks = 0;
     int row = 0;
     for (int k = 0; k < cnt; ++k) {
-      Plan* p = plans[c0 + k];
+      Plan* p = plans[ord[c0 + k]];
       const GeomParams& gp = p->gp;
       cudaMemcpy3DParms cp;
       memset(&cp, 0, sizeof(cp));
-      cp.srcPtr = make_cudaPitchedPtr((void*)sinos[c0 + k], gp.nu * sizeof(float), gp.nu, gp.nv);
+      cp.srcPtr = make_cudaPitchedPtr((void*)sinos[ord[c0 + k]], gp.nu * sizeof(float), gp.nu, gp.nv);
       cp.dstArray = p->sino_arrays[0];
       cp.extent = make_cudaExtent(gp.nu, gp.nv, gp.n_views);
       cp.kind = cudaMemcpyDeviceToDevice;
@@ -573,7 +593,7 @@ int backward_many_impl(Plan* const* plans, const float* const* sinos, float* con
       it.bp.sino_pad_elems = 0;
       it.views = p->d_bpv;
       it.tex = p->sino_tex[0];
-      it.out = outs[c0 + k];
+      it.out = outs[ord[c0 + k]];
       it.tiles = bp_tiles(gp, it.bp.vsplit);
       it.block0 = (int)blocks;
       it.zaffine = p->bp_zaffine;
@@ -587,12 +607,17 @@ int backward_many_impl(Plan* const* plans, const float* const* sinos, float* con
     }
     DTV_CHECK(blocks < 2147483647LL, "too many blocks for one launch");
     m.count = cnt;
-    bool any_split = false;
-    for (int k = 0; k < cnt; ++k) any_split |= m.it[k].bp.vsplit == 2;
-    const size_t sm = any_split ? (size_t)zc * 128 * sizeof(float) : 0;
-    if (zc == 8) bp_many_kernel<8><<<(unsigned)blocks, kBPThreads, sm, st>>>(m, accumulate);
-    else if (zc == 4) bp_many_kernel<4><<<(unsigned)blocks, kBPThreads, sm, st>>>(m, accumulate);
-    else bp_many_kernel<2><<<(unsigned)blocks, kBPThreads, sm, st>>>(m, accumulate);
+    const unsigned nb = (unsigned)blocks;
+    if (kind == 2) {
+      const size_t sm = (size_t)zc * 128 * sizeof(float);
+      if (zc == 8) bp_many_kernel<8, true><<<nb, kBPThreads, sm, st>>>(m, accumulate);
+      else if (zc == 4) bp_many_kernel<4, true><<<nb, kBPThreads, sm, st>>>(m, accumulate);
+      else bp_many_kernel<2, true><<<nb, kBPThreads, sm, st>>>(m, accumulate);
+    } else {
+      if (zc == 8) bp_many_kernel<8, false><<<nb, kBPThreads, 0, st>>>(m, accumulate);
+      else if (zc == 4) bp_many_kernel<4, false><<<nb, kBPThreads, 0, st>>>(m, accumulate);
+      else bp_many_kernel<2, false><<<nb, kBPThreads, 0, st>>>(m, accumulate);
+    }
     note_launch();
     DTV_LAUNCH_CHECK();
     c0 += cnt;
