@@ -201,7 +201,7 @@ def op_profile(plan, alg, img, sino, dev):
     import dtvb200
     from dtvb200 import _lib
     from dtvb200.geometry import _ptr, _stream
-    key = (tuple(img.shape), img.device.index, alg._fused())
+    key = (tuple(img.shape), img.device.index, alg._fused(), alg.defer_clip)
     st = alg._state[key]
     prm = alg._params()
     size = _lib.ivec(plan.geometry.volume_size)
@@ -226,12 +226,18 @@ def op_profile(plan, alg, img, sino, dev):
         e[1].record(stream)
         plan.backward(st["w"], out=st["recon"])
         e[2].record(stream)
-        _lib.call("dtv_pdhg_dual", _ptr(fbar), _ptr(st["p"]), _ptr(st["q"]), _ptr(st["s"]),
-                  _ptr(st["c"]), size, 1, ctypes.byref(prm), _ptr(st["t"]), _ptr(st["ws"]),
-                  _stream(dev))
-        _lib.call("dtv_pdhg_primal", _ptr(f), _ptr(fbar), _ptr(st["recon"]), _ptr(st["p"]),
-                  _ptr(st["q"]), _ptr(st["s"]), _ptr(st["c"]), size, 1, ctypes.byref(prm),
-                  _ptr(st["ws"]), _stream(dev))
+        # the update steps as DTVCP runs them: the duals' clip deferred into
+        # the next dual step, the last primal step storing it
+        duals = (_ptr(st["p"]), _ptr(st["q"]), _ptr(st["s"]), _ptr(st["c"]), size, 1,
+                 ctypes.byref(prm))
+        _lib.call("dtv_pdhg_dual_defer", _ptr(fbar), *duals, _ptr(st["t"]), _ptr(st["ws"]),
+                  _ptr(st["carry"]) if it > 0 else None, _stream(dev))
+        if it == alg.cascades - 1:
+            _lib.call("dtv_pdhg_primal", _ptr(f), _ptr(fbar), _ptr(st["recon"]), *duals,
+                      _ptr(st["ws"]), _stream(dev))
+        else:
+            _lib.call("dtv_pdhg_primal_defer", _ptr(f), _ptr(fbar), _ptr(st["recon"]), *duals,
+                      _ptr(st["ws"]), _ptr(st["carry"]), _stream(dev))
         e[3].record(stream)
         pairs.append(e)
     torch.cuda.synchronize()

@@ -582,13 +582,28 @@ __global__ void l1_apply_kernel(const float* __restrict__ v, float* __restrict__
 // Slices per thread of the dual step (its duals of all slices are held in
 // registers before any store, so fewer slices mean more resident blocks).
 constexpr int kDualZS = 4;
+// clip(x, m) = sign(x) * min(|x|, m): the duals' projection by the L1-ball
+// threshold m. Wherever the result compares equal to x it has x's own bits
+// (-0 included: the sign is copied from x), so storing it in place of an
+// unclipped element changes no memory.
+__device__ __forceinline__ float clipf(float x, float m) { return copysignf(fminf(fabsf(x), m), x); }
+
+// The thresholds a deferred clip applies to the duals a dual step loads:
+// those the previous primal step clipped with (carry), or +inf (no clip).
+__device__ __forceinline__ float carry_thresh(const float* carry, int a) {
+  return carry ? carry[a] : __int_as_float(0x7f800000);
+}
+
 template <class T>
 __global__ void __launch_bounds__(256, 6) pdhg_dual_kernel(const T* __restrict__ fbar, float* __restrict__ p,
                                                         float* __restrict__ q, float* __restrict__ s,
                                                         float* __restrict__ c, Dims d, float a0,
                                                         float a1, float a2, float smu,
-                                                        L1Chan* chans, int64_t n_tiles) {
+                                                        L1Chan* chans, int64_t n_tiles,
+                                                        const float* carry) {
   __shared__ unsigned int hs[3][3 * kL1B1];
+  const float m0 = carry_thresh(carry, 0), m1 = carry_thresh(carry, 1),
+              m2 = carry_thresh(carry, 2);
   for (int i = ltid(); i < 9 * kL1B1; i += lthreads()) (&hs[0][0])[i] = 0u;
   __syncthreads();
   unsigned int kmax[3] = {0u, 0u, 0u};
@@ -610,9 +625,9 @@ __global__ void __launch_bounds__(256, 6) pdhg_dual_kernel(const T* __restrict__
     pv[k] = qv[k] = sv[k] = cv[k] = 0.f;
     if (cl.in && k < cl.nz) {
       const int64_t t = cl.base + i0 + k * plane;
-      pv[k] = p[t];
-      qv[k] = q[t];
-      sv[k] = s[t];
+      pv[k] = clipf(p[t], m0);
+      qv[k] = clipf(q[t], m1);
+      sv[k] = clipf(s[t], m2);
       cv[k] = c[t];
     }
   }
@@ -679,6 +694,9 @@ __device__ __forceinline__ float4 load4_as_float(const __nv_bfloat16* p, int64_t
   const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w.y));
   return make_float4(a.x, a.y, b.x, b.y);
 }
+__device__ __forceinline__ float4 clip4(float4 v, float m) {
+  return make_float4(clipf(v.x, m), clipf(v.y, m), clipf(v.z, m), clipf(v.w, m));
+}
 __device__ __forceinline__ float4 f4_zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
 
 // The same dual step with four consecutive x per thread: the duals move as
@@ -697,9 +715,11 @@ __global__ void __launch_bounds__(256, 4) pdhg_dual_x4_kernel(const T* __restric
                                                            float* __restrict__ c, Dims d,
                                                            float a0, float a1, float a2,
                                                            float smu, L1Chan* chans,
-                                                           int n_tiles) {
+                                                           int n_tiles, const float* carry) {
   __shared__ unsigned int hs[3][3 * kL1B1];
+  __shared__ float msh[3];  // thresholds of the deferred clip
   for (int i = ltid(); i < 9 * kL1B1; i += lthreads()) (&hs[0][0])[i] = 0u;
+  if (ltid() < 3) msh[ltid()] = carry_thresh(carry, ltid());
   __syncthreads();
   unsigned int kmax[3] = {0u, 0u, 0u};
   const int tx = (d.X + kX4TX - 1) / kX4TX, ty = (d.Y + kTY - 1) / kTY;
@@ -722,9 +742,9 @@ __global__ void __launch_bounds__(256, 4) pdhg_dual_x4_kernel(const T* __restric
       P[k] = Q[k] = S[k] = C[k] = f4_zero();
       if (in && k < nz) {
         const int64_t t = base + i0 + k * plane;
-        P[k] = *reinterpret_cast<const float4*>(p + t);
-        Q[k] = *reinterpret_cast<const float4*>(q + t);
-        S[k] = *reinterpret_cast<const float4*>(s + t);
+        P[k] = clip4(*reinterpret_cast<const float4*>(p + t), msh[0]);
+        Q[k] = clip4(*reinterpret_cast<const float4*>(q + t), msh[1]);
+        S[k] = clip4(*reinterpret_cast<const float4*>(s + t), msh[2]);
         C[k] = *reinterpret_cast<const float4*>(c + t);
       }
     }
@@ -749,7 +769,8 @@ __global__ void __launch_bounds__(256, 4) pdhg_dual_x4_kernel(const T* __restric
       const float qs[4] = {Q[k].x, Q[k].y, Q[k].z, Q[k].w};
       const float ss[4] = {S[k].x, S[k].y, S[k].z, S[k].w};
       const float cs[4] = {C[k].x, C[k].y, C[k].z, C[k].w};
-      float np[4], nq[4], ns[4];
+      float np[4], nq[4], ns[4], cw[4];
+      bool cc = false;
       const int64_t t = base + i;
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
@@ -758,10 +779,14 @@ __global__ void __launch_bounds__(256, 4) pdhg_dual_x4_kernel(const T* __restric
         np[e] = fmaf(a0, gxs[e], ps[e]);
         nq[e] = fmaf(a1, gy, qs[e]);
         ns[e] = fmaf(a2, gz, ss[e]);
-        // -relu(-c - sigma*mu*fbar): stays 0 wherever fbar >= 0, stored only on change
+        // -relu(-c - sigma*mu*fbar): stays 0 wherever fbar >= 0; a vector is
+        // stored only if one of its elements changes, the others keeping
+        // their own bytes
         const float cn = fminf(fmaf(smu, fcs[e], cs[e]), 0.f);
-        if (cn != cs[e]) c[t + e] = cn;
+        cc |= cn != cs[e];
+        cw[e] = cn != cs[e] ? cn : cs[e];
       }
+      if (cc) *reinterpret_cast<float4*>(c + t) = make_float4(cw[0], cw[1], cw[2], cw[3]);
       *reinterpret_cast<float4*>(p + t) = make_float4(np[0], np[1], np[2], np[3]);
       *reinterpret_cast<float4*>(q + t) = make_float4(nq[0], nq[1], nq[2], nq[3]);
       *reinterpret_cast<float4*>(s + t) = make_float4(ns[0], ns[1], ns[2], ns[3]);
@@ -790,7 +815,6 @@ __global__ void __launch_bounds__(256, 4) pdhg_dual_x4_kernel(const T* __restric
   }
 }
 
-__device__ __forceinline__ float clipf(float x, float m) { return copysignf(fminf(fabsf(x), m), x); }
 
 // ---- fused PDHG primal step (DTVCP.py:44-54) ----------------------------------------------------
 // The duals are clipped in place; neighbours may read a value before or after
@@ -801,10 +825,15 @@ __global__ void __launch_bounds__(256) pdhg_primal_kernel(float* __restrict__ f,
                                                           float* q, float* s,
                                                           const float* __restrict__ c, Dims d,
                                                           float tau, float mu, float v0, float v1,
-                                                          float v2, const L1Chan* chans) {
+                                                          float v2, const L1Chan* chans,
+                                                          float* carry) {
+  const float m0 = chans[0].thresh, m1 = chans[1].thresh, m2 = chans[2].thresh;
+  // carry: the clipped duals are not stored; the thresholds go to carry, and
+  // the next dual step clips the duals as it loads them
+  if (carry && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && ltid() < 3)
+    carry[ltid()] = chans[ltid()].thresh;
   const Col cl = col3(d);
   if (!cl.in) return;
-  const float m0 = chans[0].thresh, m1 = chans[1].thresh, m2 = chans[2].thresh;
   const int64_t plane = (int64_t)d.X * d.Y;
   const int64_t oy = axis_off(d, 1);
   float* pb = p + cl.base;
@@ -821,9 +850,11 @@ __global__ void __launch_bounds__(256) pdhg_primal_kernel(float* __restrict__ f,
     if (yv) dy += clipf(qb[i - oy], m1);
     if (cl.z0 + k >= 1) dz += sprev;
     // only clipped duals change; the others keep their bytes without a store
-    if (ps != pr) pb[i] = ps;
-    if (qs != qr) qb[i] = qs;
-    if (ss != sr) sb[i] = ss;
+    if (!carry) {
+      if (ps != pr) pb[i] = ps;
+      if (qs != qr) qb[i] = qs;
+      if (ss != sr) sb[i] = ss;
+    }
     sprev = ss;
     const int64_t t = cl.base + i;
     const float reg = fmaf(v0, dx, fmaf(v1, dy, fmaf(v2, dz, mu * c[t])));
@@ -861,14 +892,16 @@ __device__ __forceinline__ void store4_from_float(__nv_bfloat16* p, int64_t i, f
 // others from the thread's own vector. Same arithmetic per voxel as
 // pdhg_primal_kernel.
 template <class T>
-__global__ void __launch_bounds__(256) pdhg_primal_x4_kernel(float* __restrict__ f,
+__global__ void __launch_bounds__(256, 4) pdhg_primal_x4_kernel(float* __restrict__ f,
                                                              T* __restrict__ fbar,
                                                              const float* __restrict__ recon,
                                                              float* p, float* q, float* s,
                                                              const float* __restrict__ c, Dims d,
                                                              float tau, float mu, float v0,
                                                              float v1, float v2,
-                                                             const L1Chan* chans) {
+                                                             const L1Chan* chans, float* carry) {
+  if (carry && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && ltid() < 3)
+    carry[ltid()] = chans[ltid()].thresh;
   const int x0 = (blockIdx.x * kTX + (int)threadIdx.x) * 4;
   const int y = blockIdx.y * kTY + (int)threadIdx.y;
   const int zslabs = (d.Z + d.zs - 1) / d.zs;
@@ -916,6 +949,23 @@ __global__ void __launch_bounds__(256) pdhg_primal_x4_kernel(float* __restrict__
       qn[2] = clipf(Qn.z, m1); qn[3] = clipf(Qn.w, m1);
     }
     const bool zv = z0 + k >= 1;
+    // only vectors with a clipped dual are stored, as one 16-byte store. An
+    // unclipped element's clip has its own bits (clipf), so the store writes
+    // the same memory as element stores would, and a neighbour reading
+    // concurrently sees the value or its clip, which are equal. With carry
+    // nothing is stored: the next dual step clips the duals as it loads them.
+    if (!carry) {
+      bool cp = false, cq = false, cs_ = false;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        cp |= ps[e] != pr[e];
+        cq |= qs[e] != qr[e];
+        cs_ |= ss[e] != sr[e];
+      }
+      if (cp) *reinterpret_cast<float4*>(pb + i) = make_float4(ps[0], ps[1], ps[2], ps[3]);
+      if (cq) *reinterpret_cast<float4*>(qb + i) = make_float4(qs[0], qs[1], qs[2], qs[3]);
+      if (cs_) *reinterpret_cast<float4*>(sb + i) = make_float4(ss[0], ss[1], ss[2], ss[3]);
+    }
     float fn[4], fb[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
@@ -924,10 +974,6 @@ __global__ void __launch_bounds__(256) pdhg_primal_x4_kernel(float* __restrict__
       else if (x0 >= 1) dx += pl;
       if (yv) dy += qn[e];
       if (zv) dz += sprev[e];
-      // only clipped duals change; the others keep their bytes without a store
-      if (ps[e] != pr[e]) pb[i + e] = ps[e];
-      if (qs[e] != qr[e]) qb[i + e] = qs[e];
-      if (ss[e] != sr[e]) sb[i + e] = ss[e];
       sprev[e] = ss[e];
       const float reg = fmaf(v0, dx, fmaf(v1, dy, fmaf(v2, dz, mu * cs[e])));
       fn[e] = fmaf(-tau, reg, fo[e] - rc[e]);
@@ -1209,9 +1255,9 @@ int dtv_l1ball(const float* v, float* w, int64_t n, const double* radius, void* 
 
 int64_t dtv_pdhg_workspace_bytes(void) { return (int64_t)(3 * sizeof(L1Chan)); }
 
-int dtv_pdhg_dual(const void* fbar, float* p, float* q, float* s, float* c, const int32_t size[3],
-                  int32_t batch, const dtv_pdhg_params* prm, const double* t, void* ws,
-                  void* stream) {
+static int pdhg_dual_impl(const void* fbar, float* p, float* q, float* s, float* c,
+                          const int32_t size[3], int32_t batch, const dtv_pdhg_params* prm,
+                          const double* t, void* ws, const float* carry, void* stream) {
   DTV_CHECK(fbar && p && q && s && c && size && prm && t && ws, "NULL argument");
   DTV_CHECK(prm->f_dtype == DTV_F32 || prm->f_dtype == DTV_F16 || prm->f_dtype == DTV_BF16,
             "f_dtype must be f32, f16 or bf16");
@@ -1250,26 +1296,26 @@ int dtv_pdhg_dual(const void* fbar, float* p, float* q, float* s, float* c, cons
     const float b0 = prm->v[0] * sg, b1 = prm->v[1] * sg, b2 = prm->v[2] * sg, sm = sg * prm->mu;
     if (prm->f_dtype == DTV_F32)
       pdhg_dual_x4_kernel<float><<<g4, kBlock3, 0, st>>>((const float*)fbar, p, q, s, c, d, b0,
-                                                          b1, b2, sm, ch, (int)t4);
+                                                          b1, b2, sm, ch, (int)t4, carry);
     else if (prm->f_dtype == DTV_F16)
       pdhg_dual_x4_kernel<__half><<<g4, kBlock3, 0, st>>>((const __half*)fbar, p, q, s, c, d, b0,
-                                                           b1, b2, sm, ch, (int)t4);
+                                                           b1, b2, sm, ch, (int)t4, carry);
     else
       pdhg_dual_x4_kernel<__nv_bfloat16><<<g4, kBlock3, 0, st>>>(
-          (const __nv_bfloat16*)fbar, p, q, s, c, d, b0, b1, b2, sm, ch, (int)t4);
+          (const __nv_bfloat16*)fbar, p, q, s, c, d, b0, b1, b2, sm, ch, (int)t4, carry);
     note_launch();
   } else if (prm->f_dtype == DTV_F32) {
     pdhg_dual_kernel<float><<<grid, kBlock3, 0, st>>>(
         (const float*)fbar, p, q, s, c, dd, prm->v[0] * sg, prm->v[1] * sg, prm->v[2] * sg,
-        sg * prm->mu, ch, tiles); note_launch();
+        sg * prm->mu, ch, tiles, carry); note_launch();
   } else if (prm->f_dtype == DTV_F16) {
     pdhg_dual_kernel<__half><<<grid, kBlock3, 0, st>>>(
         (const __half*)fbar, p, q, s, c, dd, prm->v[0] * sg, prm->v[1] * sg, prm->v[2] * sg,
-        sg * prm->mu, ch, tiles); note_launch();
+        sg * prm->mu, ch, tiles, carry); note_launch();
   } else {
     pdhg_dual_kernel<__nv_bfloat16><<<grid, kBlock3, 0, st>>>(
         (const __nv_bfloat16*)fbar, p, q, s, c, dd, prm->v[0] * sg, prm->v[1] * sg,
-        prm->v[2] * sg, sg * prm->mu, ch, tiles); note_launch();
+        prm->v[2] * sg, sg * prm->mu, ch, tiles, carry); note_launch();
   }
   DTV_LAUNCH_CHECK();
   // the shared-memory limit is a per-device function attribute
@@ -1294,9 +1340,10 @@ int dtv_pdhg_dual(const void* fbar, float* p, float* q, float* s, float* c, cons
   return DTV_OK;
 }
 
-int dtv_pdhg_primal(float* f, void* fbar, const float* recon, float* p, float* q, float* s,
-                    const float* c, const int32_t size[3], int32_t batch,
-                    const dtv_pdhg_params* prm, const void* ws, void* stream) {
+static int pdhg_primal_impl(float* f, void* fbar, const float* recon, float* p, float* q,
+                            float* s, const float* c, const int32_t size[3], int32_t batch,
+                            const dtv_pdhg_params* prm, const void* ws, float* carry,
+                            void* stream) {
   DTV_CHECK(f && fbar && recon && p && q && s && c && size && prm && ws, "NULL argument");
   DTV_CHECK(prm->f_dtype == DTV_F32 || prm->f_dtype == DTV_F16 || prm->f_dtype == DTV_BF16,
             "f_dtype must be f32, f16 or bf16");
@@ -1324,31 +1371,57 @@ int dtv_pdhg_primal(float* f, void* fbar, const float* recon, float* p, float* q
     if (prm->f_dtype == DTV_F32)
       pdhg_primal_x4_kernel<float><<<g4, kBlock3, 0, st>>>(f, (float*)fbar, recon, p, q, s, c,
                                                            d4, prm->tau, prm->mu, prm->v[0],
-                                                           prm->v[1], prm->v[2], ch);
+                                                           prm->v[1], prm->v[2], ch, carry);
     else if (prm->f_dtype == DTV_F16)
       pdhg_primal_x4_kernel<__half><<<g4, kBlock3, 0, st>>>(f, (__half*)fbar, recon, p, q, s, c,
                                                             d4, prm->tau, prm->mu, prm->v[0],
-                                                            prm->v[1], prm->v[2], ch);
+                                                            prm->v[1], prm->v[2], ch, carry);
     else
       pdhg_primal_x4_kernel<__nv_bfloat16><<<g4, kBlock3, 0, st>>>(
           f, (__nv_bfloat16*)fbar, recon, p, q, s, c, d4, prm->tau, prm->mu, prm->v[0],
-          prm->v[1], prm->v[2], ch);
+          prm->v[1], prm->v[2], ch, carry);
     note_launch();
   } else if (prm->f_dtype == DTV_F32) {
     pdhg_primal_kernel<float><<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(
         f, (float*)fbar, recon, p, q, s, c, d, prm->tau, prm->mu, prm->v[0], prm->v[1],
-        prm->v[2], ch); note_launch();
+        prm->v[2], ch, carry); note_launch();
   } else if (prm->f_dtype == DTV_F16) {
     pdhg_primal_kernel<__half><<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(
         f, (__half*)fbar, recon, p, q, s, c, d, prm->tau, prm->mu, prm->v[0], prm->v[1],
-        prm->v[2], ch); note_launch();
+        prm->v[2], ch, carry); note_launch();
   } else {
     pdhg_primal_kernel<__nv_bfloat16><<<grid3(d, batch), kBlock3, 0, as_stream(stream)>>>(
         f, (__nv_bfloat16*)fbar, recon, p, q, s, c, d, prm->tau, prm->mu, prm->v[0], prm->v[1],
-        prm->v[2], ch); note_launch();
+        prm->v[2], ch, carry); note_launch();
   }
   DTV_LAUNCH_CHECK();
   return DTV_OK;
+}
+
+int dtv_pdhg_dual(const void* fbar, float* p, float* q, float* s, float* c, const int32_t size[3],
+                  int32_t batch, const dtv_pdhg_params* prm, const double* t, void* ws,
+                  void* stream) {
+  return pdhg_dual_impl(fbar, p, q, s, c, size, batch, prm, t, ws, nullptr, stream);
+}
+
+int dtv_pdhg_dual_defer(const void* fbar, float* p, float* q, float* s, float* c,
+                        const int32_t size[3], int32_t batch, const dtv_pdhg_params* prm,
+                        const double* t, void* ws, const float* carry, void* stream) {
+  return pdhg_dual_impl(fbar, p, q, s, c, size, batch, prm, t, ws, carry, stream);
+}
+
+int dtv_pdhg_primal(float* f, void* fbar, const float* recon, float* p, float* q, float* s,
+                    const float* c, const int32_t size[3], int32_t batch,
+                    const dtv_pdhg_params* prm, const void* ws, void* stream) {
+  return pdhg_primal_impl(f, fbar, recon, p, q, s, c, size, batch, prm, ws, nullptr, stream);
+}
+
+int dtv_pdhg_primal_defer(float* f, void* fbar, const float* recon, float* p, float* q,
+                          float* s, const float* c, const int32_t size[3], int32_t batch,
+                          const dtv_pdhg_params* prm, const void* ws, float* carry,
+                          void* stream) {
+  DTV_CHECK(carry, "NULL argument");
+  return pdhg_primal_impl(f, fbar, recon, p, q, s, c, size, batch, prm, ws, carry, stream);
 }
 
 int dtv_fista_update(float* y, float* x_prev, const float* bp, int64_t n, float L, float thresh,

@@ -103,6 +103,10 @@ SIGNATURES = {
     "dtv_pdhg_dual": [_P, _P, _P, _P, _P, _IP, _I, ctypes.POINTER(dtv_pdhg_params), _P, _P, _P],
     "dtv_pdhg_primal": [_P, _P, _P, _P, _P, _P, _P, _IP, _I, ctypes.POINTER(dtv_pdhg_params),
                         _P, _P],
+    "dtv_pdhg_dual_defer": [_P, _P, _P, _P, _P, _IP, _I, ctypes.POINTER(dtv_pdhg_params), _P, _P,
+                            _P, _P],
+    "dtv_pdhg_primal_defer": [_P, _P, _P, _P, _P, _P, _P, _IP, _I,
+                              ctypes.POINTER(dtv_pdhg_params), _P, _P, _P],
     "dtv_fista_update": [_P, _P, _P, _L, _F, _F, _F, _P],
     "dtv_relu_step": [_P, _P, _P, _L, _F, _P],
     "dtv_dtvfista_maxes": [_P, _IP, _I, _FP, _P, _P],

@@ -173,6 +173,9 @@ class DTVCP(_Graphable):
                 raise ValueError("correction intervals must be at least 1")
         self.exact = exact
         self.unfused = False  # True: the correction passes as separate launches
+        # True: each primal step leaves the duals unclipped and the next dual
+        # step clips them as it loads them (same bits, no clip stores)
+        self.defer_clip = True
         self.correct_every = int(correct_every)
         self.correct_bp_every = int(correct_bp_every) if correct_bp_every else int(correct_every)
         self.plan = plan
@@ -230,6 +233,7 @@ class DTVCP(_Graphable):
             "g": torch.empty(plan.sino_shape(b), dtype=torch.float32, device=dev),
             "t": torch.zeros(3, dtype=torch.float64, device=dev),
             "loss": torch.zeros(self.cascades, dtype=torch.float64, device=dev),
+            "carry": torch.zeros(3, dtype=torch.float32, device=dev),
             "ws": torch.zeros(_lib.load().dtv_pdhg_workspace_bytes(), dtype=torch.uint8,
                               device=dev),
         }
@@ -293,17 +297,28 @@ class DTVCP(_Graphable):
                     plan.backward(st["w"], out=st["recon"], base=st["e_b"])
             else:
                 plan.adjoint(st["w"], out=st["recon"])
-            call("dtv_pdhg_dual", _ptr(fbar), _ptr(st["p"]), _ptr(st["q"]), _ptr(st["s"]),
-                 _ptr(st["c"]), size, b, ctypes.byref(prm), _ptr(st["t"]), _ptr(st["ws"]),
-                 stream)
-            call("dtv_pdhg_primal", _ptr(f), _ptr(fbar), _ptr(st["recon"]), _ptr(st["p"]),
-                 _ptr(st["q"]), _ptr(st["s"]), _ptr(st["c"]), size, b, ctypes.byref(prm),
-                 _ptr(st["ws"]), stream)
+            duals = (_ptr(st["p"]), _ptr(st["q"]), _ptr(st["s"]), _ptr(st["c"]), size, b,
+                     ctypes.byref(prm))
+            if not self.defer_clip:
+                call("dtv_pdhg_dual", _ptr(fbar), *duals, _ptr(st["t"]), _ptr(st["ws"]), stream)
+                call("dtv_pdhg_primal", _ptr(f), _ptr(fbar), _ptr(st["recon"]), *duals,
+                     _ptr(st["ws"]), stream)
+                continue
+            # the clip of iteration it-1's primal step happens as this dual
+            # step loads the duals; the last primal step stores its clip
+            call("dtv_pdhg_dual_defer", _ptr(fbar), *duals, _ptr(st["t"]), _ptr(st["ws"]),
+                 _ptr(st["carry"]) if it > 0 else None, stream)
+            if it == self.cascades - 1:
+                call("dtv_pdhg_primal", _ptr(f), _ptr(fbar), _ptr(st["recon"]), *duals,
+                     _ptr(st["ws"]), stream)
+            else:
+                call("dtv_pdhg_primal_defer", _ptr(f), _ptr(fbar), _ptr(st["recon"]), *duals,
+                     _ptr(st["ws"]), _ptr(st["carry"]), stream)
 
     def _prepare(self, image, sino):
         check_input(image, "image", self.plan.vol_shape(image.shape[0]),
                     dtypes=(torch.float32, torch.float16, torch.bfloat16))
-        key = (tuple(image.shape), image.device.index, self._fused())
+        key = (tuple(image.shape), image.device.index, self._fused(), self.defer_clip)
         st = self.__dict__.setdefault("_state", {}).get(key)
         if st is None:
             st = self._alloc(image)

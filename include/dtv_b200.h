@@ -395,6 +395,28 @@ DTV_API int dtv_pdhg_dual(const void* fbar, float* p, float* q, float* s, float*
 DTV_API int dtv_pdhg_primal(float* f, void* fbar, const float* recon, float* p, float* q, float* s,
                     const float* c, const int32_t size[3], int32_t batch,
                     const dtv_pdhg_params* prm, const void* workspace, void* stream);
+/* The same two steps with the duals' clip deferred from one iteration's
+ * primal step into the next iteration's dual step, which loads the duals
+ * anyway. No counterpart in the reference (an iteration of DTVCP.py:38-54
+ * split differently).
+ * dtv_pdhg_primal_defer computes f and fbar as dtv_pdhg_primal does but
+ * stores no clipped dual: p, q, s keep the values dtv_pdhg_dual left, and
+ * the three thresholds it clipped them with are written to carry (device
+ * float[3], not in the workspace).
+ * dtv_pdhg_dual_defer is dtv_pdhg_dual on the duals clipped to carry as it
+ * loads them (carry NULL: no clip, the same as dtv_pdhg_dual).
+ * A clip leaves an unclipped element's bits unchanged, so an iteration
+ * sequence of dual_defer(carry) / primal_defer(carry) gives the bits of
+ * dtv_pdhg_dual / dtv_pdhg_primal; ending it with dtv_pdhg_primal leaves the
+ * same clipped duals too. */
+DTV_API int dtv_pdhg_dual_defer(const void* fbar, float* p, float* q, float* s, float* c,
+                                const int32_t size[3], int32_t batch, const dtv_pdhg_params* prm,
+                                const double* t, void* workspace, const float* carry,
+                                void* stream);
+DTV_API int dtv_pdhg_primal_defer(float* f, void* fbar, const float* recon, float* p, float* q,
+                                  float* s, const float* c, const int32_t size[3], int32_t batch,
+                                  const dtv_pdhg_params* prm, const void* workspace, float* carry,
+                                  void* stream);
 
 /* ---- FISTA (model/FISTA/FISTA.py:16-27) ------------------------------------------ */
 /* d = y - L*bp; x = sign(d)*max(|d| - thresh, 0); y = x + momentum*(x - x_prev);
