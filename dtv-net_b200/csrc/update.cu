@@ -293,6 +293,29 @@ __device__ __forceinline__ void hist_add(unsigned int* h, int nb, int bin, unsig
   atomicAdd(h + 2 * nb + bin, sig >> 12);
 }
 
+// Four elements (a thread's four consecutive x in the four-x dual step): one
+// add of all four when they are active and share a bin, else one add each.
+// The duals of a reconstruction concentrate in a few bins as the iterations
+// go on (clipped to a common bound, then moved by one small step), and lanes
+// adding to one shared-memory word serialise; neighbours usually share their
+// bin then. The four significands sum to S < 2^26, added as S mod 2^12 to the low word and
+// S / 2^12 to the high word: the flushed sum low + high * 2^12 is the same
+// integer, and the high word's adds still total at most the block's
+// significand sum / 2^12 < 2^32.
+__device__ __forceinline__ void hist_add4(unsigned int* h, int nb, const int (&bin)[4],
+                                          const unsigned int (&key)[4], const bool (&act)[4]) {
+  if (act[0] && act[1] && act[2] && act[3] && bin[0] == bin[1] && bin[1] == bin[2] &&
+      bin[2] == bin[3]) {
+    const unsigned int S = sig24(key[0]) + sig24(key[1]) + sig24(key[2]) + sig24(key[3]);
+    atomicAdd(h + bin[0], 4u);
+    atomicAdd(h + nb + bin[0], S & 0xFFFu);
+    atomicAdd(h + 2 * nb + bin[0], S >> 12);
+    return;
+  }
+#pragma unroll
+  for (int e = 0; e < 4; ++e) hist_add(h, nb, bin[e], key[e], act[e]);
+}
+
 __device__ __forceinline__ void hist_clear(unsigned int* h, int nb) {
   for (int i = ltid(); i < 3 * nb; i += lthreads()) h[i] = 0u;
 }
@@ -790,17 +813,19 @@ __global__ void __launch_bounds__(256, 4) pdhg_dual_x4_kernel(const T* __restric
       *reinterpret_cast<float4*>(p + t) = make_float4(np[0], np[1], np[2], np[3]);
       *reinterpret_cast<float4*>(q + t) = make_float4(nq[0], nq[1], nq[2], nq[3]);
       *reinterpret_cast<float4*>(s + t) = make_float4(ns[0], ns[1], ns[2], ns[3]);
+      const bool all[4] = {true, true, true, true};
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const unsigned int k0 = __float_as_uint(np[e]) & 0x7FFFFFFFu;
-        const unsigned int k1 = __float_as_uint(nq[e]) & 0x7FFFFFFFu;
-        const unsigned int k2 = __float_as_uint(ns[e]) & 0x7FFFFFFFu;
-        kmax[0] = max(kmax[0], k0);
-        kmax[1] = max(kmax[1], k1);
-        kmax[2] = max(kmax[2], k2);
-        hist_add(hs[0], kL1B1, (int)(k0 >> kL1S1), k0, true);
-        hist_add(hs[1], kL1B1, (int)(k1 >> kL1S1), k1, true);
-        hist_add(hs[2], kL1B1, (int)(k2 >> kL1S1), k2, true);
+      for (int a = 0; a < 3; ++a) {
+        const float* nv = a == 0 ? np : (a == 1 ? nq : ns);
+        unsigned int k[4];
+        int b[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          k[e] = __float_as_uint(nv[e]) & 0x7FFFFFFFu;
+          b[e] = (int)(k[e] >> kL1S1);
+          kmax[a] = max(kmax[a], k[e]);
+        }
+        hist_add4(hs[a], kL1B1, b, k, all);
       }
       fc = fn;
     }
