@@ -153,6 +153,13 @@ class DTVCP(_Graphable):
     exact operators themselves. ``correct_bp_every`` sets the backprojector's
     refresh interval apart (default: ``correct_every``); 1 backprojects with
     the exact plan in every iteration.
+
+    The duals' clip to the L1-ball thresholds (:44-47) is deferred: each
+    primal step but the last leaves p, q, s unclipped and keeps its three
+    thresholds on the device, and the next dual step clips the duals as it
+    loads them (dtv_pdhg_primal_defer / dtv_pdhg_dual_defer). Late in a
+    reconstruction most duals are clipped, and this saves storing them; the
+    result has the same bits. ``defer_clip = False`` runs the storing steps.
     """
 
     def __init__(self, plan: Plan, cascades: int = 30, sigma: float = 1e-7, tau: float = 1e-7,
