@@ -112,6 +112,11 @@ def test_null_arguments_are_rejected():
     assert L.dtv_pdhg_forward_refresh(None, None, None, 0, 1, None, 0.0, None, None, None,
                                       None) == 1
     assert L.dtv_backward_refresh(None, None, None, 1, None, None, None) == 1
+    assert L.dtv_pdhg_dual_defer(None, None, None, None, None, None, 1, None, None, None, None,
+                                 None) == 1
+    assert L.dtv_pdhg_primal_defer(None, None, None, None, None, None, None, None, 1, None, None,
+                                   None, None) == 1
+    assert b"NULL" in L.dtv_last_error_message()
 
 
 def test_check_input_errors():
