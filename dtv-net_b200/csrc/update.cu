@@ -298,10 +298,10 @@ __device__ __forceinline__ void hist_add(unsigned int* h, int nb, int bin, unsig
 // The duals of a reconstruction concentrate in a few bins as the iterations
 // go on (clipped to a common bound, then moved by one small step), and lanes
 // adding to one shared-memory word serialise; neighbours usually share their
-// bin then. The four significands sum to S < 2^26, added as S mod 2^12 to the low word and
-// S / 2^12 to the high word: the flushed sum low + high * 2^12 is the same
-// integer, and the high word's adds still total at most the block's
-// significand sum / 2^12 < 2^32.
+// bin then. The four significands sum to S < 2^26, added as S mod 2^12 to
+// the low word and S / 2^12 to the high word: the flushed sum
+// low + high * 2^12 is the same integer, and the high word's adds still
+// total at most the block's significand sum / 2^12 < 2^32.
 __device__ __forceinline__ void hist_add4(unsigned int* h, int nb, const int (&bin)[4],
                                           const unsigned int (&key)[4], const bool (&act)[4]) {
   if (act[0] && act[1] && act[2] && act[3] && bin[0] == bin[1] && bin[1] == bin[2] &&
@@ -840,10 +840,10 @@ __global__ void __launch_bounds__(256, 4) pdhg_dual_x4_kernel(const T* __restric
   }
 }
 
-
 // ---- fused PDHG primal step (DTVCP.py:44-54) ----------------------------------------------------
-// The duals are clipped in place; neighbours may read a value before or after
-// its clip, and clipping is idempotent, so both give the same result.
+// Without carry the duals are clipped in place; neighbours may read a value
+// before or after its clip, and clipping is idempotent, so both give the same
+// result. With carry (the deferred clip) they are only read.
 template <class T>
 __global__ void __launch_bounds__(256) pdhg_primal_kernel(float* __restrict__ f, T* __restrict__ fbar,
                                                           const float* __restrict__ recon, float* p,
